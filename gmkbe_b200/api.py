@@ -1,0 +1,223 @@
+"""Python host mirror of the enumerator's C ABI (include/gmk.h), via ctypes.
+
+    g = gmkbe_b200.Graph.load("g.graph.bin", device=0)
+    st = g.enumerate(k=1, result_limit=10**6)
+    st.count, st.hash_sum, st.hash_xor
+
+Argument meanings and errors follow the reference executable (-f/-k/-r/-d,
+src/main.cu:1719-1775): k >= 1, a result limit of 0 means "all", a CUDA or
+file error raises GmkError.  There is no CPU path: without libgmk.so or a
+GPU, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libgmk.so")
+
+# entry points declared in include/gmk.h
+EXPORTS = ("gmk_graph_load", "gmk_graph_from_csr", "gmk_graph_info", "gmk_graph_free",
+           "gmk_opts_default", "gmk_enumerate", "gmk_result_hash", "gmk_strerror",
+           "gmk_last_cuda_error", "gmk_abi_version")
+
+SCHEDULES = {"plain": 0, "batched": 1, "ordered": 2}
+
+E_OUTBUF = -9
+E_SINK = -10
+
+
+class GmkError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"gmk error {code}: {msg}")
+        self.code = code
+
+
+class _Opts(ctypes.Structure):
+    _fields_ = [("k", ctypes.c_uint32), ("result_limit", ctypes.c_uint64),
+                ("schedule", ctypes.c_int32), ("emit", ctypes.c_int32),
+                ("chunk", ctypes.c_uint32), ("threads", ctypes.c_uint32),
+                ("arena_words", ctypes.c_uint32), ("max_members", ctypes.c_uint32),
+                ("watchdog_ms", ctypes.c_uint32), ("out_words", ctypes.c_uint64),
+                ("task_cost", ctypes.POINTER(ctypes.c_float)), ("pair_limit", ctypes.c_uint32),
+                ("shard", ctypes.c_uint32), ("nshards", ctypes.c_uint32)]
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [("count", ctypes.c_uint64), ("hash_sum", ctypes.c_uint64),
+                ("hash_xor", ctypes.c_uint64), ("nodes", ctypes.c_uint64),
+                ("algo_bytes", ctypes.c_uint64), ("tasks", ctypes.c_uint64),
+                ("tasks_done", ctypes.c_uint64), ("kernel_ms", ctypes.c_double),
+                ("truncated", ctypes.c_int32), ("threads", ctypes.c_uint32)]
+
+
+SINK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32),
+                        ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint32)
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libgmk.so; raises if it is missing (no fallback exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise GmkError(-11, f"{path} not built; run `python -m gmkbe_b200.build`")
+    lib = ctypes.CDLL(path)
+    P32 = ctypes.POINTER(ctypes.c_uint32)
+    lib.gmk_graph_load.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+    lib.gmk_graph_from_csr.argtypes = [P32, P32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_void_p)]
+    lib.gmk_graph_info.argtypes = [ctypes.c_void_p, P32, P32, ctypes.POINTER(ctypes.c_uint64)]
+    lib.gmk_graph_free.argtypes = [ctypes.c_void_p]
+    lib.gmk_graph_free.restype = None
+    lib.gmk_opts_default.argtypes = [ctypes.POINTER(_Opts)]
+    lib.gmk_opts_default.restype = None
+    lib.gmk_enumerate.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Opts), SINK, ctypes.c_void_p,
+                                  ctypes.POINTER(_Stats)]
+    lib.gmk_result_hash.argtypes = [P32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                    ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
+    lib.gmk_result_hash.restype = None
+    lib.gmk_strerror.restype = ctypes.c_char_p
+    lib.gmk_last_cuda_error.restype = ctypes.c_char_p
+    _lib = lib
+    return lib
+
+
+def _check(rc: int) -> None:
+    if rc:
+        lib = load_library()
+        raise GmkError(rc, f"{lib.gmk_strerror(rc).decode()} ({lib.gmk_last_cuda_error().decode()})")
+
+
+@dataclass
+class Stats:
+    count: int
+    hash_sum: int
+    hash_xor: int
+    nodes: int
+    algo_bytes: int
+    tasks: int
+    tasks_done: int
+    kernel_ms: float
+    truncated: bool
+    threads: int
+    results: list | None = None
+
+    def summary(self) -> tuple[int, int, int]:
+        return self.count, self.hash_sum, self.hash_xor
+
+
+def result_hash(x, y) -> tuple[int, int]:
+    """The library's per-result hash pair (gmk_result_hash)."""
+    lib = load_library()
+    ids = np.ascontiguousarray(list(x) + list(y) or [0], dtype=np.uint32)
+    h1, h2 = ctypes.c_uint64(), ctypes.c_uint64()
+    lib.gmk_result_hash(ids.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), len(x) + len(y),
+                        len(x), len(y), ctypes.byref(h1), ctypes.byref(h2))
+    return h1.value, h2.value
+
+
+class Graph:
+    """A bipartite graph resident on one GPU (gmk_graph)."""
+
+    def __init__(self, handle: int, device: int):
+        self._h = ctypes.c_void_p(handle)
+        self.device = device
+        lib = load_library()
+        n, nl, m = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint64()
+        _check(lib.gmk_graph_info(self._h, ctypes.byref(n), ctypes.byref(nl), ctypes.byref(m)))
+        self.n, self.n_left, self.adj_len = n.value, nl.value, m.value
+
+    @classmethod
+    def load(cls, path: str, device: int = 0) -> "Graph":
+        lib = load_library()
+        h = ctypes.c_void_p()
+        _check(lib.gmk_graph_load(os.fsencode(path), device, ctypes.byref(h)))
+        return cls(h.value, device)
+
+    @classmethod
+    def from_csr(cls, offsets, adj, n: int, n_left: int, device: int = 0) -> "Graph":
+        lib = load_library()
+        off = np.ascontiguousarray(offsets, dtype=np.uint32)
+        a = np.ascontiguousarray(adj, dtype=np.uint32)
+        if a.size == 0:
+            a = np.zeros(1, np.uint32)
+        P = ctypes.POINTER(ctypes.c_uint32)
+        h = ctypes.c_void_p()
+        _check(lib.gmk_graph_from_csr(off.ctypes.data_as(P), a.ctypes.data_as(P), n, n_left,
+                                      device, ctypes.byref(h)))
+        return cls(h.value, device)
+
+    @classmethod
+    def from_graph(cls, g, device: int = 0) -> "Graph":
+        """From a gmkbe_b200.graphgen.Graph."""
+        return cls.from_csr(g.offsets, g.adj, g.n, g.n_left, device)
+
+    def close(self) -> None:
+        if self._h:
+            load_library().gmk_graph_free(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def enumerate(self, k: int = 1, result_limit: int = 0, schedule: str = "batched",
+                  collect: bool = False, chunk: int = 0, threads: int = 0, arena_words: int = 0,
+                  max_members: int = 0, watchdog_ms: int = 0, pair_limit: int = 0,
+                  task_cost=None, sink=None, shard: int = 0, nshards: int = 1) -> Stats:
+        """Enumerate maximal k-biplexes.  collect=True returns the result list
+        (sorted X, Y tuples) in Stats.results; `sink(x, y)` is called per
+        result otherwise (return True to stop)."""
+        lib = load_library()
+        o = _Opts()
+        lib.gmk_opts_default(ctypes.byref(o))
+        o.k, o.result_limit, o.schedule = k, result_limit, SCHEDULES[schedule]
+        o.chunk, o.threads, o.arena_words = chunk, threads, arena_words
+        o.max_members, o.watchdog_ms, o.pair_limit = max_members, watchdog_ms, pair_limit
+        o.shard, o.nshards = shard, nshards
+        cost = None
+        if task_cost is not None:
+            cost = np.ascontiguousarray(task_cost, dtype=np.float32)
+            if cost.size != self.n_left:
+                raise ValueError("task_cost needs one value per U vertex")
+            o.task_cost = cost.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        out: list = []
+        cb = SINK(0)
+        if collect or sink is not None:
+            o.emit = 1
+
+            def _sink(_u, xp, nx, yp, ny):
+                x = tuple(xp[i] for i in range(nx))
+                y = tuple(yp[i] for i in range(ny))
+                if collect:
+                    out.append((x, y))
+                    return 0
+                return 1 if sink(x, y) else 0
+            cb = SINK(_sink)
+        st = _Stats()
+        while True:
+            out.clear()
+            rc = lib.gmk_enumerate(self._h, ctypes.byref(o), cb, None, ctypes.byref(st))
+            if rc != E_OUTBUF:
+                break
+            o.out_words = (o.out_words or (64 << 20)) * 4
+        if rc != E_SINK:
+            _check(rc)
+        return Stats(st.count, st.hash_sum, st.hash_xor, st.nodes, st.algo_bytes, st.tasks,
+                     st.tasks_done, st.kernel_ms, bool(st.truncated), st.threads,
+                     out if collect else None)

@@ -1,0 +1,416 @@
+// libgmk.so: the C ABI of include/gmk.h over the sm_100a enumeration kernel.
+//
+// Host side: .graph.bin reading and CSR validation, device residency of the
+// graph, a cached per-graph workspace (search arenas, member buffers,
+// counters, record buffer), the persistent-kernel launch, and delivery of
+// result records to the caller's sink.  Device side: enumerate_kernel, one
+// search task per thread at a time, tasks taken from a device work queue.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/gmk.h"
+#include "enum_core.cuh"
+
+namespace {
+
+thread_local std::string g_cuda_err;
+
+int cuda_fail(cudaError_t e, const char* what) {
+    g_cuda_err = std::string(what) + ": " + cudaGetErrorString(e);
+    if (e == cudaErrorMemoryAllocation) return GMK_E_NOMEM;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return GMK_E_NODEV;
+    return GMK_E_CUDA;
+}
+
+#define CK(call)                                              \
+    do {                                                      \
+        cudaError_t e_ = (call);                              \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call);   \
+    } while (0)
+
+struct Counters {
+    unsigned long long count, hash_sum, hash_xor, nodes, work, next_task, out_pos, tasks_done;
+    int stop, error;
+};
+
+constexpr int kBlock = 128;
+constexpr uint32_t kDefaultArena = 1u << 16;
+constexpr uint32_t kDefaultSmax = 2048;
+constexpr uint32_t kDefaultPairLimit = 4096;
+
+__global__ void __launch_bounds__(kBlock)
+enumerate_kernel(gmk::GraphView g, uint32_t k, Counters* ctr, uint32_t* arenas,
+                 uint32_t arena_words, uint32_t* sbuf, uint32_t smax, uint32_t pair_limit,
+                 unsigned long long n_tasks, uint32_t chunk, uint32_t chunks_per_root,
+                 const uint32_t* root_order, unsigned long long limit, uint32_t* out_buf,
+                 unsigned long long out_cap, unsigned long long watchdog_ns, uint32_t shard,
+                 uint32_t nshards) {
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    gmk::Outputs o;
+    o.count = &ctr->count; o.hash_sum = &ctr->hash_sum; o.hash_xor = &ctr->hash_xor;
+    o.nodes = &ctr->nodes; o.work = &ctr->work; o.stop = &ctr->stop; o.error = &ctr->error;
+    o.limit = limit; o.out_buf = out_buf; o.out_pos = &ctr->out_pos; o.out_cap = out_cap;
+    o.deadline_ns = watchdog_ns ? gmk::now_ns() + watchdog_ns : 0ull;
+    gmk::Task t;
+    t.g = g; t.k = k;
+    t.arena = arenas + tid * arena_words; t.cap = arena_words;
+    t.sid = sbuf + tid * 2ull * smax; t.smc = t.sid + smax; t.smax = smax;
+    t.ns = 0; t.nss[0] = t.nss[1] = 0;
+    t.scan_limit = pair_limit; t.err = 0;
+    t.cnt = t.hsum = t.hxor = t.nodes = t.work = 0;
+    while (!gmk::load_flag(o.stop)) {
+        const unsigned long long j = atomicAdd(&ctr->next_task, 1ull);
+        const unsigned long long id = j * nshards + shard;
+        if (id >= n_tasks) break;
+        atomicAdd(&ctr->tasks_done, 1ull);
+        const uint32_t r = (uint32_t)(id / chunks_per_root);
+        const uint32_t c = (uint32_t)(id % chunks_per_root);
+        const uint32_t root = root_order ? root_order[r] : r;
+        const uint32_t first = g.nl + c * chunk;
+        const uint64_t end = (uint64_t)first + chunk;
+        const uint32_t last = end < g.n ? (uint32_t)end : g.n;
+        gmk::run_task(t, o, root, first, last);
+        gmk::flush(t, o);
+        if (t.err) break;
+    }
+    gmk::flush(t, o);
+}
+
+bool read_file(const char* path, std::vector<uint32_t>& words) {
+    FILE* fp = std::fopen(path, "rb");
+    if (!fp) return false;
+    std::fseek(fp, 0, SEEK_END);
+    long sz = std::ftell(fp);
+    std::fseek(fp, 0, SEEK_SET);
+    if (sz < 0 || sz % 4) { std::fclose(fp); return false; }
+    words.resize((size_t)sz / 4);
+    size_t got = std::fread(words.data(), 4, words.size(), fp);
+    std::fclose(fp);
+    return got == words.size();
+}
+
+// Rows must be strictly ascending and hold ids of the other side only.
+int validate_csr(const uint32_t* off, const uint32_t* adj, uint32_t n, uint32_t nl) {
+    if (nl > n || off[0] != 0) return GMK_E_FORMAT;
+    for (uint32_t v = 0; v < n; ++v) {
+        if (off[v + 1] < off[v]) return GMK_E_FORMAT;
+        const uint32_t lo = v < nl ? nl : 0u, hi = v < nl ? n : nl;
+        for (uint32_t p = off[v]; p < off[v + 1]; ++p) {
+            const uint32_t w = adj[p];
+            if (w < lo || w >= hi) return GMK_E_FORMAT;
+            if (p > off[v] && adj[p - 1] >= w) return GMK_E_FORMAT;
+        }
+    }
+    return GMK_OK;
+}
+
+}  // namespace
+
+struct gmk_graph {
+    int device = 0;
+    uint32_t n = 0, nl = 0;
+    uint64_t adj_len = 0;
+    uint32_t* d_off = nullptr;
+    uint32_t* d_adj = nullptr;
+    Counters* d_ctr = nullptr;
+    uint32_t* d_order = nullptr;
+    size_t order_bytes = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+// Search arenas, member buffers and the record buffer are large and outlive
+// any one graph: one set per device, grown on demand, kept until exit.
+// Calls on the same device are serialised by the mutex.
+struct Workspace {
+    std::mutex mu;
+    uint32_t* d_arena = nullptr;
+    size_t arena_bytes = 0;
+    uint32_t* d_sbuf = nullptr;
+    size_t sbuf_bytes = 0;
+    uint32_t* d_out = nullptr;
+    size_t out_bytes = 0;
+};
+constexpr int kMaxDevices = 64;
+Workspace g_ws[kMaxDevices];
+
+}  // namespace
+
+namespace {
+
+int grow(void** p, size_t* have, size_t need) {
+    if (*have >= need && *p) return GMK_OK;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *have = 0;
+    cudaError_t e = cudaMalloc(p, need);
+    if (e != cudaSuccess) { *p = nullptr; return cuda_fail(e, "cudaMalloc(workspace)"); }
+    *have = need;
+    return GMK_OK;
+}
+
+int upload(const uint32_t* off, const uint32_t* adj, uint32_t n, uint32_t nl, int device,
+           gmk_graph** out) {
+    int rc = validate_csr(off, adj, n, nl);
+    if (rc) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        g_cuda_err = "no CUDA device";
+        return GMK_E_NODEV;
+    }
+    if (device < 0 || device >= ndev || device >= kMaxDevices) return GMK_E_INVAL;
+    CK(cudaSetDevice(device));
+    gmk_graph* g = new (std::nothrow) gmk_graph();
+    if (!g) return GMK_E_NOMEM;
+    g->device = device; g->n = n; g->nl = nl; g->adj_len = off[n];
+    auto bail = [&](int code) { gmk_graph_free(g); return code; };
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return bail(cuda_fail(e, "cudaStreamCreate"));
+    if ((e = cudaEventCreate(&g->ev0)) != cudaSuccess || (e = cudaEventCreate(&g->ev1)) != cudaSuccess)
+        return bail(cuda_fail(e, "cudaEventCreate"));
+    if ((e = cudaMalloc(&g->d_off, sizeof(uint32_t) * (n + 1ull))) != cudaSuccess)
+        return bail(cuda_fail(e, "cudaMalloc(offsets)"));
+    if ((e = cudaMalloc(&g->d_adj, sizeof(uint32_t) * std::max<uint64_t>(1, g->adj_len))) != cudaSuccess)
+        return bail(cuda_fail(e, "cudaMalloc(adj)"));
+    if ((e = cudaMemcpyAsync(g->d_off, off, sizeof(uint32_t) * (n + 1ull), cudaMemcpyHostToDevice,
+                             g->stream)) != cudaSuccess)
+        return bail(cuda_fail(e, "H2D offsets"));
+    if (g->adj_len && (e = cudaMemcpyAsync(g->d_adj, adj, sizeof(uint32_t) * g->adj_len,
+                                           cudaMemcpyHostToDevice, g->stream)) != cudaSuccess)
+        return bail(cuda_fail(e, "H2D adj"));
+    if ((e = cudaMalloc(&g->d_ctr, sizeof(Counters))) != cudaSuccess)
+        return bail(cuda_fail(e, "cudaMalloc(counters)"));
+    if ((e = cudaStreamSynchronize(g->stream)) != cudaSuccess) return bail(cuda_fail(e, "upload"));
+    *out = g;
+    return GMK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gmk_abi_version(void) { return GMK_ABI_VERSION; }
+
+const char* gmk_last_cuda_error(void) { return g_cuda_err.c_str(); }
+
+const char* gmk_strerror(int code) {
+    switch (code) {
+        case GMK_OK: return "ok";
+        case GMK_E_INVAL: return "invalid argument";
+        case GMK_E_IO: return "cannot read input file";
+        case GMK_E_FORMAT: return "malformed graph (header, ids, sides or unsorted rows)";
+        case GMK_E_CUDA: return "CUDA runtime error";
+        case GMK_E_NOMEM: return "device out of memory";
+        case GMK_E_ARENA: return "search task outgrew its arena (raise arena_words)";
+        case GMK_E_SMAX: return "k-biplex larger than max_members";
+        case GMK_E_TIMEOUT: return "watchdog expired";
+        case GMK_E_OUTBUF: return "record buffer too small (raise out_words)";
+        case GMK_E_SINK: return "stopped by the sink";
+        case GMK_E_NODEV: return "no usable CUDA device";
+        default: return "unknown error";
+    }
+}
+
+void gmk_result_hash(const uint32_t* ids, uint32_t n_ids, uint32_t nx, uint32_t ny, uint64_t* h1,
+                     uint64_t* h2) {
+    uint64_t a = 0, b = 0;
+    for (uint32_t i = 0; i < n_ids; ++i) {
+        uint64_t e = gmk::elem_a(ids[i]);
+        a += e;
+        b += gmk::elem_b(e);
+    }
+    if (h1) *h1 = gmk::final_h1(a, nx, ny);
+    if (h2) *h2 = gmk::final_h2(b, nx, ny);
+}
+
+int gmk_graph_load(const char* path, int device, gmk_graph** out) {
+    if (!path || !out) return GMK_E_INVAL;
+    *out = nullptr;
+    std::vector<uint32_t> w;
+    if (!read_file(path, w)) return GMK_E_IO;
+    if (w.size() < 3) return GMK_E_FORMAT;
+    const uint32_t adj_len = w[0], n = w[1], nl = w[2];
+    if (nl > n) return GMK_E_FORMAT;
+    std::vector<uint32_t> off(n + 1ull, 0), adj;
+    adj.reserve(adj_len);
+    size_t pos = 3;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (pos + 2 > w.size() || w[pos] != i) return GMK_E_FORMAT;
+        const uint32_t d = w[pos + 1];
+        pos += 2;
+        if (pos + d > w.size()) return GMK_E_FORMAT;
+        adj.insert(adj.end(), w.begin() + pos, w.begin() + pos + d);
+        pos += d;
+        if (adj.size() > 0xFFFFFFFFull) return GMK_E_FORMAT;
+        off[i + 1] = (uint32_t)adj.size();
+    }
+    if (adj.size() != adj_len) return GMK_E_FORMAT;
+    return upload(off.data(), adj.data(), n, nl, device, out);
+}
+
+int gmk_graph_from_csr(const uint32_t* offsets, const uint32_t* adj, uint32_t n, uint32_t n_left,
+                       int device, gmk_graph** out) {
+    if (!offsets || !out || (!adj && offsets[n] != 0)) return GMK_E_INVAL;
+    *out = nullptr;
+    static const uint32_t none = 0;
+    return upload(offsets, adj ? adj : &none, n, n_left, device, out);
+}
+
+int gmk_graph_info(const gmk_graph* g, uint32_t* n, uint32_t* n_left, uint64_t* adj_len) {
+    if (!g) return GMK_E_INVAL;
+    if (n) *n = g->n;
+    if (n_left) *n_left = g->nl;
+    if (adj_len) *adj_len = g->adj_len;
+    return GMK_OK;
+}
+
+void gmk_graph_free(gmk_graph* g) {
+    if (!g) return;
+    cudaSetDevice(g->device);
+    if (g->stream) cudaStreamSynchronize(g->stream);
+    cudaFree(g->d_off); cudaFree(g->d_adj); cudaFree(g->d_ctr); cudaFree(g->d_order);
+    if (g->ev0) cudaEventDestroy(g->ev0);
+    if (g->ev1) cudaEventDestroy(g->ev1);
+    if (g->stream) cudaStreamDestroy(g->stream);
+    delete g;
+}
+
+void gmk_opts_default(gmk_opts* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->k = 1;
+    o->schedule = GMK_SCHEDULE_BATCHED;
+}
+
+int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user, gmk_stats* out) {
+    if (!g || !opts || !out) return GMK_E_INVAL;
+    if (opts->k < 1 || opts->k > 15) return GMK_E_INVAL;
+    if (opts->emit && !sink) return GMK_E_INVAL;
+    if (opts->schedule == GMK_SCHEDULE_ORDERED && !opts->task_cost) return GMK_E_INVAL;
+    if (opts->nshards && opts->shard >= opts->nshards) return GMK_E_INVAL;
+    std::memset(out, 0, sizeof(*out));
+    CK(cudaSetDevice(g->device));
+    if (g->nl == 0 || g->n == g->nl) return GMK_OK;   // a side is empty: no k-biplex
+
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, g->device));
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, enumerate_kernel, kBlock, 0));
+    per_sm = std::max(per_sm, 1);
+    const uint32_t arena_words = opts->arena_words ? opts->arena_words : kDefaultArena;
+    const uint32_t smax = opts->max_members ? opts->max_members : kDefaultSmax;
+    uint64_t threads = opts->threads ? opts->threads
+                                     : (uint64_t)prop.multiProcessorCount * per_sm * kBlock;
+    // keep the search arenas within 40% of free device memory
+    size_t free_b = 0, total_b = 0;
+    CK(cudaMemGetInfo(&free_b, &total_b));
+    const uint64_t per_thread = 4ull * arena_words + 8ull * smax;
+    Workspace& ws = g_ws[g->device];
+    std::lock_guard<std::mutex> lock(ws.mu);
+    const uint64_t budget = (uint64_t)((double)(free_b + ws.arena_bytes + ws.sbuf_bytes) * 0.4);
+    if (threads * per_thread > budget) threads = std::max<uint64_t>(kBlock, budget / per_thread);
+    threads = (threads + kBlock - 1) / kBlock * kBlock;
+
+    // tasks: root x, chunk of first-level children
+    const uint32_t nv = g->n - g->nl;
+    uint32_t chunk = nv;
+    if (opts->schedule != GMK_SCHEDULE_PLAIN) {
+        if (opts->chunk) {
+            chunk = std::min(opts->chunk, nv);
+        } else {
+            // about 8 tasks per thread, but no chunk below 16 children
+            const uint64_t want = 8ull * threads;
+            const uint64_t per_root = (want + g->nl - 1) / g->nl;
+            chunk = (uint32_t)std::max<uint64_t>(16, (nv + per_root - 1) / std::max<uint64_t>(1, per_root));
+            chunk = std::min(chunk, nv);
+        }
+    }
+    const uint32_t chunks_per_root = (nv + chunk - 1) / chunk;
+    const unsigned long long n_tasks = (unsigned long long)g->nl * chunks_per_root;
+
+    int rc;
+    if ((rc = grow((void**)&ws.d_arena, &ws.arena_bytes, threads * 4ull * arena_words))) return rc;
+    if ((rc = grow((void**)&ws.d_sbuf, &ws.sbuf_bytes, threads * 8ull * smax))) return rc;
+    const uint32_t* d_order = nullptr;
+    if (opts->schedule == GMK_SCHEDULE_ORDERED) {
+        std::vector<uint32_t> order(g->nl);
+        std::iota(order.begin(), order.end(), 0u);
+        const float* cost = opts->task_cost;
+        std::stable_sort(order.begin(), order.end(),
+                         [cost](uint32_t a, uint32_t b) { return cost[a] > cost[b]; });
+        if ((rc = grow((void**)&g->d_order, &g->order_bytes, 4ull * g->nl))) return rc;
+        CK(cudaMemcpyAsync(g->d_order, order.data(), 4ull * g->nl, cudaMemcpyHostToDevice, g->stream));
+        d_order = g->d_order;
+    }
+    uint64_t out_words = 0;
+    if (opts->emit) {
+        out_words = opts->out_words ? opts->out_words : (64ull << 20);
+        if ((rc = grow((void**)&ws.d_out, &ws.out_bytes, out_words * 4ull))) return rc;
+    }
+    CK(cudaMemsetAsync(g->d_ctr, 0, sizeof(Counters), g->stream));
+    gmk::GraphView gv{g->d_off, g->d_adj, g->n, g->nl};
+    const unsigned grid = (unsigned)(threads / kBlock);
+    CK(cudaEventRecord(g->ev0, g->stream));
+    enumerate_kernel<<<grid, kBlock, 0, g->stream>>>(
+        gv, opts->k, g->d_ctr, ws.d_arena, arena_words, ws.d_sbuf, smax,
+        opts->pair_limit ? opts->pair_limit : kDefaultPairLimit, n_tasks, chunk, chunks_per_root,
+        d_order, opts->result_limit, opts->emit ? ws.d_out : nullptr, out_words,
+        (unsigned long long)opts->watchdog_ms * 1000000ull, opts->nshards ? opts->shard : 0u,
+        opts->nshards ? opts->nshards : 1u);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(g->ev1, g->stream));
+    Counters h;
+    CK(cudaMemcpyAsync(&h, g->d_ctr, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
+    CK(cudaStreamSynchronize(g->stream));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
+
+    out->count = opts->result_limit ? std::min<unsigned long long>(h.count, opts->result_limit) : h.count;
+    out->hash_sum = h.hash_sum;
+    out->hash_xor = h.hash_xor;
+    out->nodes = h.nodes;
+    out->algo_bytes = 4ull * h.work;
+    const uint32_t nsh = opts->nshards ? opts->nshards : 1u, sh = opts->nshards ? opts->shard : 0u;
+    out->tasks = n_tasks > sh ? (n_tasks - sh + nsh - 1) / nsh : 0;
+    out->tasks_done = std::min<unsigned long long>(h.tasks_done, out->tasks);
+    out->kernel_ms = ms;
+    out->truncated = opts->result_limit && h.count >= opts->result_limit;
+    out->threads = (uint32_t)threads;
+    switch (h.error) {
+        case gmk::TASK_OK: break;
+        case gmk::TASK_E_ARENA: return GMK_E_ARENA;
+        case gmk::TASK_E_SMAX: return GMK_E_SMAX;
+        case gmk::TASK_E_TIMEOUT: return GMK_E_TIMEOUT;
+        default: return GMK_E_CUDA;
+    }
+    if (opts->emit) {
+        if (h.out_pos > out_words) return GMK_E_OUTBUF;
+        std::vector<uint32_t> rec(h.out_pos);
+        if (h.out_pos)
+            CK(cudaMemcpy(rec.data(), ws.d_out, 4ull * h.out_pos, cudaMemcpyDeviceToHost));
+        size_t p = 0;
+        while (p + 2 <= rec.size()) {
+            const uint32_t nx = rec[p], ny = rec[p + 1];
+            uint32_t* x = rec.data() + p + 2;
+            uint32_t* y = x + nx;
+            std::sort(x, x + nx);
+            std::sort(y, y + ny);
+            if (sink(user, x, nx, y, ny)) return GMK_E_SINK;
+            p += 2ull + nx + ny;
+        }
+    }
+    return GMK_OK;
+}
+
+}  // extern "C"

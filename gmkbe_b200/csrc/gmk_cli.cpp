@@ -1,0 +1,105 @@
+// gmk: drop-in command line for the reference's `gmkbpe` executable.
+//
+// Same flags as reference src/main.cu:1719-1775:
+//   -f <file.graph.bin>  -k <k> (default 1)  -r <result limit> (default 1e7)
+//   -q <print results, 0/1> (default 0)  -d <device> (default 0)
+//   -m / -g are accepted and ignored (verbose dump / unused group size).
+// Output: "Result N: X: x1 x2 | Y: y1 y2 " lines when -q 1 (format of
+// reference include/output.cuh:102-145), then "Running Time: <ms> ms".
+// Extra: --all (no result limit), --schedule plain|batched, --stats.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+#include "gmk.h"
+
+namespace {
+
+struct Printer {
+    unsigned long long n = 0;
+};
+
+int print_result(void* user, const uint32_t* x, uint32_t nx, const uint32_t* y, uint32_t ny) {
+    Printer* p = static_cast<Printer*>(user);
+    std::printf("Result %llu: X:", ++p->n);
+    for (uint32_t i = 0; i < nx; ++i) std::printf(" %u", x[i]);
+    std::printf(" | Y: ");
+    for (uint32_t i = 0; i < ny; ++i) std::printf("%u ", y[i]);
+    std::printf("\n");
+    return 0;
+}
+
+void usage() {
+    std::fprintf(stderr,
+                 "usage: gmk -f <graph.bin> [-k K] [-r LIMIT] [-q 0|1] [-d DEV] [--all]\n"
+                 "           [--schedule plain|batched] [--stats]\n");
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    std::string file;
+    gmk_opts o;
+    gmk_opts_default(&o);
+    o.result_limit = 10000000ull;
+    int quiet = 0, dev = 0, stats = 0;
+    for (int i = 1; i < argc; ++i) {
+        auto val = [&](const char* name) -> const char* {
+            if (i + 1 >= argc) { std::fprintf(stderr, "missing value for %s\n", name); std::exit(2); }
+            return argv[++i];
+        };
+        if (!std::strcmp(argv[i], "-f")) file = val("-f");
+        else if (!std::strcmp(argv[i], "-k")) o.k = (uint32_t)std::strtoul(val("-k"), nullptr, 10);
+        else if (!std::strcmp(argv[i], "-r")) o.result_limit = std::strtoull(val("-r"), nullptr, 10);
+        else if (!std::strcmp(argv[i], "-q")) quiet = std::atoi(val("-q"));
+        else if (!std::strcmp(argv[i], "-d")) dev = std::atoi(val("-d"));
+        else if (!std::strcmp(argv[i], "-m") || !std::strcmp(argv[i], "-g")) (void)val(argv[i]);
+        else if (!std::strcmp(argv[i], "--all")) o.result_limit = 0;
+        else if (!std::strcmp(argv[i], "--stats")) stats = 1;
+        else if (!std::strcmp(argv[i], "--schedule")) {
+            const char* s = val("--schedule");
+            o.schedule = !std::strcmp(s, "plain") ? GMK_SCHEDULE_PLAIN : GMK_SCHEDULE_BATCHED;
+        } else if (!std::strcmp(argv[i], "-h") || !std::strcmp(argv[i], "--help")) {
+            usage();
+            return 0;
+        } else {
+            usage();
+            return 2;
+        }
+    }
+    if (file.empty()) { usage(); return 2; }
+    gmk_graph* g = nullptr;
+    int rc = gmk_graph_load(file.c_str(), dev, &g);
+    if (rc) {
+        std::fprintf(stderr, "gmk: %s (%s)\n", gmk_strerror(rc), gmk_last_cuda_error());
+        return 1;
+    }
+    uint32_t n = 0, nl = 0;
+    uint64_t m = 0;
+    gmk_graph_info(g, &n, &nl, &m);
+    std::printf("Graph size: %u, edge num: %llu, bipartite index: %u, k = %u\n", n,
+                (unsigned long long)m, nl, o.k);
+    Printer p;
+    o.emit = quiet ? 1 : 0;
+    gmk_stats st;
+    for (;;) {
+        rc = gmk_enumerate(g, &o, quiet ? print_result : nullptr, &p, &st);
+        if (rc != GMK_E_OUTBUF) break;
+        o.out_words = (o.out_words ? o.out_words : (64ull << 20)) * 4;   // retry, bigger buffer
+        p.n = 0;
+    }
+    if (rc) {
+        std::fprintf(stderr, "gmk: %s (%s)\n", gmk_strerror(rc), gmk_last_cuda_error());
+        gmk_graph_free(g);
+        return 1;
+    }
+    std::printf("Running Time: %.3f ms\n", st.kernel_ms);
+    if (stats)
+        std::printf("results %llu hash_sum %016llx hash_xor %016llx nodes %llu tasks %llu threads %u\n",
+                    (unsigned long long)st.count, (unsigned long long)st.hash_sum,
+                    (unsigned long long)st.hash_xor, (unsigned long long)st.nodes,
+                    (unsigned long long)st.tasks, st.threads);
+    gmk_graph_free(g);
+    return 0;
+}

@@ -1,0 +1,126 @@
+/* gmk.h -- C ABI of the B200 maximal k-biplex enumerator (libgmk.so).
+ *
+ * The reference (GMkBPE) has no library API: its boundary is the `gmkbpe`
+ * executable.  Each entry point below replaces one step of that executable so
+ * that a host program (C, C++, Python ctypes, Go cgo, ...) can drive the same
+ * path without a process boundary.  Plain pointers and sizes only.
+ *
+ * Graph ids follow the `.graph.bin` numbering: U = [0, n_left), V = [n_left, n).
+ * Results are maximal k-biplexes (X in U, Y in V, both non-empty).
+ * All functions return GMK_OK (0) or a negative GMK_E* code; gmk_strerror()
+ * names it.  A gmk_graph may not be used by two gmk_enumerate calls at once.
+ */
+#ifndef GMK_H
+#define GMK_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GMK_ABI_VERSION 1
+
+enum {
+    GMK_OK = 0,
+    GMK_E_INVAL = -1,    /* bad argument */
+    GMK_E_IO = -2,       /* cannot open / read the file */
+    GMK_E_FORMAT = -3,   /* malformed .graph.bin or CSR (ids, sides, unsorted rows) */
+    GMK_E_CUDA = -4,     /* CUDA runtime error (message via gmk_last_cuda_error) */
+    GMK_E_NOMEM = -5,    /* device allocation failed */
+    GMK_E_ARENA = -6,    /* a search task outgrew its arena; raise arena_words */
+    GMK_E_SMAX = -7,     /* a k-biplex larger than max_members */
+    GMK_E_TIMEOUT = -8,  /* watchdog_ms elapsed; counts cover the work done so far */
+    GMK_E_OUTBUF = -9,   /* record buffer too small for emit mode; raise out_words */
+    GMK_E_SINK = -10,    /* the sink asked to stop (not an error for the caller's data) */
+    GMK_E_NODEV = -11    /* no CUDA device / extension not usable */
+};
+
+typedef struct gmk_graph gmk_graph;
+
+/* Replaces: load_graph_from_bin (reference data/src/tmp_load.h:213-295) plus
+ * the CSR upload of testEnumerate (reference src/main.cu:1680-1690).
+ * Reads a .graph.bin file and makes the CSR resident on `device`. */
+int gmk_graph_load(const char* path, int device, gmk_graph** out);
+
+/* Same, from caller-owned host CSR arrays (copied; the caller keeps them).
+ * offsets: n+1 entries; adj: offsets[n] global ids, each row sorted ascending,
+ * U rows hold V ids and V rows hold U ids. */
+int gmk_graph_from_csr(const uint32_t* offsets, const uint32_t* adj, uint32_t n,
+                       uint32_t n_left, int device, gmk_graph** out);
+
+/* Sizes of a loaded graph (any pointer may be NULL). */
+int gmk_graph_info(const gmk_graph* g, uint32_t* n, uint32_t* n_left, uint64_t* adj_len);
+
+/* Releases device memory (the CSR and any cached enumeration workspace). */
+void gmk_graph_free(gmk_graph* g);
+
+/* Schedules of the search tasks (one task = a root U vertex and a chunk of its
+ * first-level children). */
+enum {
+    GMK_SCHEDULE_PLAIN = 0,    /* one task per root, roots in id order */
+    GMK_SCHEDULE_BATCHED = 1,  /* roots split into chunks, persistent work queue */
+    GMK_SCHEDULE_ORDERED = 2   /* batched, tasks ordered by a caller-given cost (longest first) */
+};
+
+typedef struct {
+    uint32_t k;               /* -k: misses allowed per vertex (>= 1) */
+    uint64_t result_limit;    /* -r: stop after this many results; 0 = enumerate all */
+    int32_t schedule;         /* GMK_SCHEDULE_* */
+    int32_t emit;             /* 0: count + set hash only; 1: also deliver every result to the sink */
+    uint32_t chunk;           /* first-level children per task (batched); 0 = automatic */
+    uint32_t threads;         /* resident search threads; 0 = automatic */
+    uint32_t arena_words;     /* per-thread search arena (u32 words); 0 = automatic */
+    uint32_t max_members;     /* largest |X|+|Y| a task may hold; 0 = 2048 */
+    uint32_t watchdog_ms;     /* stop with GMK_E_TIMEOUT after this long; 0 = none */
+    uint64_t out_words;       /* emit-mode record buffer (u32 words); 0 = automatic */
+    const float* task_cost;   /* GMK_SCHEDULE_ORDERED: one cost per root U vertex (n_left) */
+    uint32_t pair_limit;      /* node rules (shortcut, forcing, exclusion prune) run while
+                                 (|S|+|C_U|)*(|S|+|C_V|) <= pair_limit; 0 = 4096 */
+    uint32_t shard, nshards;  /* run only tasks t with t % nshards == shard (one GPU of
+                                 several); nshards 0 or 1 = all tasks */
+} gmk_opts;
+
+typedef struct {
+    uint64_t count;           /* results (clamped to result_limit) */
+    uint64_t hash_sum;        /* wrapping sum of per-result h1 (exact only when not truncated) */
+    uint64_t hash_xor;        /* xor of per-result h2 (exact only when not truncated) */
+    uint64_t nodes;           /* search-tree nodes */
+    uint64_t algo_bytes;      /* adjacency/counter bytes the search read (4 per word) */
+    uint64_t tasks;           /* search tasks in the queue */
+    uint64_t tasks_done;      /* tasks taken from the queue */
+    double kernel_ms;         /* device time of the enumeration kernel (CUDA events) */
+    int32_t truncated;        /* 1 if result_limit stopped the search */
+    uint32_t threads;         /* search threads used */
+} gmk_stats;
+
+/* Called from the calling thread after the kernel finished, once per result;
+ * x and y hold global ids sorted ascending.  Return non-zero to stop. */
+typedef int (*gmk_sink)(void* user, const uint32_t* x, uint32_t nx, const uint32_t* y,
+                        uint32_t ny);
+
+/* Fills *o with the defaults (k = 1, no limit, batched schedule). */
+void gmk_opts_default(gmk_opts* o);
+
+/* Replaces: enumerate_GPU (reference src/main.cu:999-1580) with everything it
+ * calls -- Generate_GPU (include/for_generate.cuh:300-512), ListBFS2_GPU
+ * (include/for_BFS.cuh:463-777), Special_GPU (include/for_special.cuh:274-683)
+ * and the CheckMaximality family (include/for_checkmaximality.cuh) -- and the
+ * result printer (include/output.cuh:93-150) when emit = 1.
+ * Enumerates the maximal k-biplexes of g on its device. */
+int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
+                  gmk_stats* out);
+
+/* Canonical per-result hash pair (the set summary's h1/h2): ids are the
+ * global ids of X u Y in any order, nx = |X|, ny = |Y|.  Host-only. */
+void gmk_result_hash(const uint32_t* ids, uint32_t n_ids, uint32_t nx, uint32_t ny,
+                     uint64_t* h1, uint64_t* h2);
+
+const char* gmk_strerror(int code);
+const char* gmk_last_cuda_error(void);
+int gmk_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GMK_H */

@@ -1,0 +1,182 @@
+"""Parity of the CUDA enumerator (through the C ABI) with the oracle and with
+the golden summaries of the reference's BPPivot output."""
+import os
+
+import numpy as np
+import pytest
+
+import gmkbe_b200 as G
+import oracle as O
+from gmkbe_b200 import graphgen as gg
+from conftest import GOLDEN, golden_graph_path
+
+pytestmark = pytest.mark.gpu
+
+
+def _summary(case):
+    return case["count"], int(case["hash_sum"], 16), int(case["hash_xor"], 16)
+
+
+@pytest.fixture(scope="module")
+def graphs():
+    cache = {}
+
+    def get(name):
+        if name not in cache:
+            cache[name] = G.Graph.load(golden_graph_path(name))
+        return cache[name]
+    yield get
+    for g in cache.values():
+        g.close()
+
+
+GOLDEN_CASES = [("southernwomen", 1), ("southernwomen", 2), ("southernwomen", 3), ("crime", 1),
+                ("er200", 1), ("cl20k_sub", 1), ("er60", 1), ("er60", 2)]
+
+
+@pytest.mark.parametrize("name,k", GOLDEN_CASES)
+def test_golden_full_enumeration(golden, graphs, name, k):
+    case = next(c for c in golden["cases"] if c["graph"] == name and c["k"] == k)
+    st = graphs(name).enumerate(k=k)
+    assert not st.truncated
+    assert st.summary() == _summary(case)
+
+
+@pytest.mark.parametrize("schedule,chunk", [("plain", 0), ("batched", 1), ("batched", 3),
+                                            ("batched", 64)])
+def test_schedule_does_not_change_the_set(golden, graphs, schedule, chunk):
+    case = next(c for c in golden["cases"] if c["graph"] == "southernwomen" and c["k"] == 2)
+    st = graphs("southernwomen").enumerate(k=2, schedule=schedule, chunk=chunk)
+    assert st.summary() == _summary(case)
+
+
+def test_ordered_schedule_same_set(golden, graphs):
+    case = next(c for c in golden["cases"] if c["graph"] == "er60" and c["k"] == 2)
+    g = graphs("er60")
+    cost = np.random.default_rng(0).random(g.n_left).astype(np.float32)
+    st = g.enumerate(k=2, schedule="ordered", task_cost=cost)
+    assert st.summary() == _summary(case)
+
+
+def test_thread_and_arena_shapes_do_not_change_the_set(golden, graphs):
+    case = next(c for c in golden["cases"] if c["graph"] == "er200" and c["k"] == 1)
+    for threads, pair_limit in [(128, 1), (1024, 64), (0, 1 << 20)]:
+        st = graphs("er200").enumerate(k=1, threads=threads, pair_limit=pair_limit)
+        assert st.summary() == _summary(case), (threads, pair_limit)
+
+
+def test_emitted_sets_equal_reference_sets(graphs):
+    want = []
+    with open(os.path.join(GOLDEN, "southernwomen_k1_sets.txt")) as f:
+        for line in f:
+            xs, ys = line.split("|")
+            want.append((tuple(map(int, xs.split())), tuple(map(int, ys.split()))))
+    st = graphs("southernwomen").enumerate(k=1, collect=True)
+    assert sorted(st.results) == sorted(want)
+
+
+@pytest.mark.parametrize("k", [1, 2, 3])
+def test_random_graphs_against_oracle(k):
+    for seed in range(12):
+        rng = np.random.default_rng(100 + seed)
+        nu, nv = int(rng.integers(3, 25)), int(rng.integers(3, 25))
+        g = gg.erdos_renyi(nu, nv, float(rng.uniform(0.1, 0.5)), 100 + seed)
+        if g.n_left in (0, g.n):
+            continue
+        want = O.enumerate_oracle(g, k).summary()
+        with G.Graph.from_graph(g) as dg:
+            got = dg.enumerate(k=k, chunk=int(rng.integers(1, 6))).summary()
+        assert got == want, (seed, k)
+
+
+def test_chung_lu_small_against_oracle():
+    g = gg.chung_lu(400, 700, 1500, 2.1, 11, max_deg=80)
+    want = O.enumerate_oracle(g, 1).summary()
+    with G.Graph.from_graph(g) as dg:
+        assert dg.enumerate(k=1).summary() == want
+
+
+# ---------------------------------------------------------------- edge cases
+
+def test_single_edge():
+    g = gg.relabel(np.array([0]), np.array([0]))
+    with G.Graph.from_graph(g) as dg:
+        st = dg.enumerate(k=1, collect=True)
+    assert st.results == [((0,), (1,))]
+
+
+def test_complete_bipartite_is_one_result():
+    u, v = np.meshgrid(np.arange(6), np.arange(5), indexing="ij")
+    g = gg.relabel(u.ravel(), v.ravel())
+    for k in (1, 2, 3):
+        with G.Graph.from_graph(g) as dg:
+            st = dg.enumerate(k=k, collect=True)
+        assert st.results == [(tuple(range(6)), tuple(range(6, 11)))]
+
+
+def test_star_and_matching_against_definition():
+    # a star plus a perfect matching: many disconnected maximal 1-biplexes
+    u = np.array([0, 0, 0, 0, 1, 2, 3, 4])
+    v = np.array([0, 1, 2, 3, 4, 5, 6, 7])
+    g = gg.relabel(u, v)
+    for k in (1, 2):
+        want = sorted(O.brute_force(g, k)) if g.n <= 16 else None
+        with G.Graph.from_graph(g) as dg:
+            got = sorted(dg.enumerate(k=k, collect=True).results)
+        assert got == want
+
+
+def test_empty_side_has_no_results():
+    off = np.zeros(4, np.uint32)          # three U vertices, no V, no edges
+    with G.Graph.from_csr(off, np.zeros(0, np.uint32), 3, 3) as dg:
+        assert dg.enumerate(k=1).count == 0
+
+
+def test_bad_csr_rejected():
+    off = np.array([0, 1, 2], np.uint32)
+    adj = np.array([0, 0], np.uint32)     # U vertex 0 adjacent to itself: not bipartite
+    with pytest.raises(G.GmkError) as e:
+        G.Graph.from_csr(off, adj, 2, 1)
+    assert e.value.code == -3
+
+
+def test_result_limit_exact_in_record_mode(graphs):
+    st = graphs("er200").enumerate(k=1, result_limit=5000, collect=True)
+    assert st.count == 5000 and len(st.results) == 5000 and st.truncated
+    g = gg.read_graph_bin(golden_graph_path("er200"))
+    for x, y in st.results[::250]:
+        assert O.classify(g, 1, x, y) == 2
+
+
+def test_result_limit_count_mode(graphs):
+    st = graphs("er200").enumerate(k=1, result_limit=100000)
+    assert st.count == 100000 and st.truncated
+
+
+def test_small_arena_reports_error_not_fault(graphs):
+    with pytest.raises(G.GmkError) as e:
+        graphs("er200").enumerate(k=1, arena_words=40)
+    assert e.value.code == -6
+    # the context stays usable
+    assert graphs("er60").enumerate(k=1).count == 8041
+
+
+def test_watchdog_returns_status():
+    g = gg.erdos_renyi(300, 300, 0.05, 5)
+    with G.Graph.from_graph(g) as dg:
+        with pytest.raises(G.GmkError) as e:
+            dg.enumerate(k=3, watchdog_ms=20)
+        assert e.value.code == -8
+        assert dg.enumerate(k=1, result_limit=10).count == 10
+
+
+def test_limited_run_at_full_size():
+    path = gg.cached_workload("cl20k")
+    with G.Graph.load(path) as dg:
+        st = dg.enumerate(k=1, result_limit=1_000_000)
+        assert st.count == 1_000_000 and st.truncated
+        sample = dg.enumerate(k=1, result_limit=2000, collect=True)
+    g = gg.read_graph_bin(path)
+    assert len(set(sample.results)) == 2000
+    for x, y in sample.results[::100]:
+        assert O.classify(g, 1, x, y) == 2

@@ -26,6 +26,7 @@ EXPORTS = ("gmk_graph_load", "gmk_graph_from_csr", "gmk_graph_info", "gmk_graph_
            "gmk_last_cuda_error", "gmk_abi_version")
 
 SCHEDULES = {"plain": 0, "batched": 1, "ordered": 2}
+ENGINES = {"warp": 0, "thread": 1}
 
 E_OUTBUF = -9
 E_SINK = -10
@@ -44,7 +45,8 @@ class _Opts(ctypes.Structure):
                 ("arena_words", ctypes.c_uint32), ("max_members", ctypes.c_uint32),
                 ("watchdog_ms", ctypes.c_uint32), ("out_words", ctypes.c_uint64),
                 ("task_cost", ctypes.POINTER(ctypes.c_float)), ("pair_limit", ctypes.c_uint32),
-                ("shard", ctypes.c_uint32), ("nshards", ctypes.c_uint32)]
+                ("shard", ctypes.c_uint32), ("nshards", ctypes.c_uint32),
+                ("engine", ctypes.c_int32), ("split_min_nodes", ctypes.c_uint32)]
 
 
 class _Stats(ctypes.Structure):
@@ -52,7 +54,8 @@ class _Stats(ctypes.Structure):
                 ("hash_xor", ctypes.c_uint64), ("nodes", ctypes.c_uint64),
                 ("algo_bytes", ctypes.c_uint64), ("tasks", ctypes.c_uint64),
                 ("tasks_done", ctypes.c_uint64), ("kernel_ms", ctypes.c_double),
-                ("truncated", ctypes.c_int32), ("threads", ctypes.c_uint32)]
+                ("truncated", ctypes.c_int32), ("threads", ctypes.c_uint32),
+                ("rounds", ctypes.c_uint32)]
 
 
 SINK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32),
@@ -107,6 +110,7 @@ class Stats:
     kernel_ms: float
     truncated: bool
     threads: int
+    rounds: int = 1
     results: list | None = None
 
     def summary(self) -> tuple[int, int, int]:
@@ -179,7 +183,8 @@ class Graph:
     def enumerate(self, k: int = 1, result_limit: int = 0, schedule: str = "batched",
                   collect: bool = False, chunk: int = 0, threads: int = 0, arena_words: int = 0,
                   max_members: int = 0, watchdog_ms: int = 0, pair_limit: int = 0,
-                  task_cost=None, sink=None, shard: int = 0, nshards: int = 1) -> Stats:
+                  task_cost=None, sink=None, shard: int = 0, nshards: int = 1,
+                  engine: str = "warp", split_min_nodes: int = 0) -> Stats:
         """Enumerate maximal k-biplexes.  collect=True returns the result list
         (sorted X, Y tuples) in Stats.results; `sink(x, y)` is called per
         result otherwise (return True to stop)."""
@@ -190,6 +195,7 @@ class Graph:
         o.chunk, o.threads, o.arena_words = chunk, threads, arena_words
         o.max_members, o.watchdog_ms, o.pair_limit = max_members, watchdog_ms, pair_limit
         o.shard, o.nshards = shard, nshards
+        o.engine, o.split_min_nodes = ENGINES[engine], split_min_nodes
         cost = None
         if task_cost is not None:
             cost = np.ascontiguousarray(task_cost, dtype=np.float32)
@@ -219,5 +225,5 @@ class Graph:
         if rc != E_SINK:
             _check(rc)
         return Stats(st.count, st.hash_sum, st.hash_xor, st.nodes, st.algo_bytes, st.tasks,
-                     st.tasks_done, st.kernel_ms, bool(st.truncated), st.threads,
+                     st.tasks_done, st.kernel_ms, bool(st.truncated), st.threads, st.rounds,
                      out if collect else None)

@@ -1,0 +1,1046 @@
+// Warp-cooperative maximal k-biplex search (sm_100a device code).
+//
+// One warp runs one search task at a time.  The search is the one in
+// enum_core.cuh -- same frames, same node rules (shortcut, forcing, exclusion
+// prune, leaf test), same child order -- so the emitted set is identical; what
+// changes is how a node's work is spread over the 32 lanes:
+//   * every loop over a long dimension (a candidate list, a CSR row, the
+//     members of S) runs one element per lane, with ballot-based compaction
+//     so that child lists keep the parent's order and are written coalesced;
+//   * the short dimension (the members an element is tested against) runs
+//     sequentially per lane, all lanes in lockstep, so those reads broadcast;
+//   * adjacency is one probe of a device edge hash table (one 32-byte bucket
+//     almost always) instead of a binary search over a CSR row -- the
+//     reference's membership test is binarySearch over sorted rows,
+//     include/gpu_utils.cuh:258-282;
+//   * the search state (frames, lists, S) lives in a per-warp arena, so the
+//     hot part of 4-10k warps' state stays in L2 instead of 150k threads'.
+// Work that outgrows its warp is split: when the task queue of a round is
+// empty, a busy warp writes every frame that still has unexplored children
+// (plus its current node) as separate tasks for the next round.  Together
+// they cover exactly the unexplored part of its search tree.
+#pragma once
+#include "enum_core.cuh"
+
+namespace gmk {
+namespace warp {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+constexpr uint32_t kSrcCap = 17;          // k + 1 sources, k <= 16
+constexpr uint32_t FL_ROOT = 16u;         // frame flag: the task's root frame
+constexpr unsigned long long kEmptyKey = ~0ull;
+
+// Open-addressing set of edges, keys (u << 32 | v) with u in U, v in V, in
+// buckets of four 8-byte keys (one 32-byte sector).  Keys fill a bucket left
+// to right and spill to the next bucket, so an empty slot ends a search.
+struct EdgeHash {
+    const unsigned long long* slots;
+    unsigned long long bmask;   // buckets - 1 (a power of two)
+};
+
+__device__ __forceinline__ unsigned long long edge_key(uint32_t a, uint32_t b) {
+    return a < b ? ((unsigned long long)a << 32) | b : ((unsigned long long)b << 32) | a;
+}
+
+__device__ __forceinline__ unsigned long long bucket_of(unsigned long long key,
+                                                        unsigned long long bmask) {
+    return mix64(key) & bmask;
+}
+
+__device__ __noinline__ bool has_edge_tail(const EdgeHash& h, unsigned long long key,
+                                           unsigned long long bk) {
+    for (unsigned long long it = 0; it < h.bmask; ++it) {
+        bk = (bk + 1) & h.bmask;
+        const ulonglong2* p = reinterpret_cast<const ulonglong2*>(h.slots + bk * 4);
+        const ulonglong2 x = __ldg(p), y = __ldg(p + 1);
+        if (x.x == key || x.y == key || y.x == key || y.y == key) return true;
+        if (x.x == kEmptyKey || x.y == kEmptyKey || y.x == kEmptyKey || y.y == kEmptyKey)
+            return false;
+    }
+    return false;
+}
+
+__device__ __forceinline__ bool has_edge(const EdgeHash& h, uint32_t a, uint32_t b) {
+    const unsigned long long key = edge_key(a, b);
+    const unsigned long long bk = bucket_of(key, h.bmask);
+    const ulonglong2* p = reinterpret_cast<const ulonglong2*>(h.slots + bk * 4);
+    const ulonglong2 x = __ldg(p), y = __ldg(p + 1);
+    if (x.x == key || x.y == key || y.x == key || y.y == key) return true;
+    if (x.x == kEmptyKey || x.y == kEmptyKey || y.x == kEmptyKey || y.y == kEmptyKey) return false;
+    return has_edge_tail(h, key, bk);
+}
+
+// Inserts every edge of the CSR (one thread per U-row entry).
+__global__ void build_edge_hash(const uint32_t* off, const uint32_t* adj, uint32_t nl,
+                                unsigned long long* slots, unsigned long long bmask) {
+    const unsigned long long e = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t m = off[nl];
+    if (e >= m) return;
+    // row u holding entry e: the last u with off[u] <= e
+    uint32_t lo = 0, hi = nl;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (off[mid] <= e) lo = mid; else hi = mid;
+    }
+    const unsigned long long key = edge_key(lo, adj[e]);
+    unsigned long long bk = bucket_of(key, bmask);
+    for (unsigned long long it = 0; it <= bmask; ++it) {
+        for (int j = 0; j < 4; ++j) {
+            const unsigned long long prev = atomicCAS(slots + bk * 4 + j, kEmptyKey, key);
+            if (prev == kEmptyKey || prev == key) return;
+        }
+        bk = (bk + 1) & bmask;
+    }
+}
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+__device__ __forceinline__ unsigned long long warp_min64(unsigned long long v) {
+    for (int o = 16; o; o >>= 1) {
+        const unsigned long long w = __shfl_xor_sync(kFull, v, o);
+        v = w < v ? w : v;
+    }
+    return v;
+}
+__device__ __forceinline__ unsigned long long warp_sum64(unsigned long long v) {
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+template <class T>
+__device__ __forceinline__ T bcast(T v) { return __shfl_sync(kFull, v, 0); }
+
+// Next-round task list: records [ns, cnt0, cnt1, sid[ns], smc[ns],
+// frame[F_WORDS], list0[2 cnt0], list1[2 cnt1]] addressed by an index array.
+struct SplitBuf {
+    uint32_t* words;
+    unsigned long long* idx;
+    unsigned long long* used;     // words reserved
+    unsigned long long* count;    // records reserved
+    unsigned long long word_cap;
+    unsigned long long idx_cap;
+};
+
+struct Ctx {
+    GraphView g;
+    EdgeHash eh;
+    uint32_t k;
+    uint32_t* arena;
+    uint32_t cap;
+    uint32_t* sid;
+    uint32_t* smc;
+    uint32_t smax;
+    uint32_t ns, nss[2];
+    uint32_t scan_limit;
+    int err;
+    unsigned long long cnt, hsum, hxor, nodes;   // warp-uniform
+    unsigned long long work;                     // per-lane share
+    uint32_t* sat;                               // shared: kSatCap per warp
+    uint32_t* src;                               // shared: kSrcCap per warp
+    uint32_t lane;
+};
+
+__device__ __forceinline__ bool adj_test(Ctx& t, uint32_t a, uint32_t b) {
+    t.work += 2;   // one 8-byte key
+    return has_edge(t.eh, a, b);
+}
+__device__ __forceinline__ uint32_t gbit(int s) { return s ? FL_G1 : FL_G0; }
+
+// ----------------------------------------------------------------- counters
+
+__device__ void flush(Ctx& t, const Outputs& o) {
+    const unsigned long long work = warp_sum64(t.work);
+    if (t.lane == 0) {
+        if (t.cnt) {
+            const unsigned long long before = atomicAdd(o.count, t.cnt);
+            atomicAdd(o.hash_sum, t.hsum);
+            atomicXor(o.hash_xor, t.hxor);
+            if (o.limit && before + t.cnt >= o.limit) atomicExch(o.stop, 1);
+        }
+        if (t.nodes) atomicAdd(o.nodes, t.nodes);
+        if (work) atomicAdd(o.work, work);
+    }
+    t.cnt = t.hsum = t.hxor = t.nodes = 0;
+    t.work = 0;
+    __syncwarp();
+}
+
+__device__ void fail(Ctx& t, const Outputs& o, int code) {
+    if (!t.err) t.err = code;
+    if (t.lane == 0) {
+        atomicCAS(o.error, 0, code);
+        atomicExch(o.stop, 1);
+    }
+}
+
+// ----------------------------------------------------------------- members
+
+// Misses of w against the other side of S, or k+1 if w cannot join S
+// (per lane; the same test as compat_misses in enum_core.cuh).
+__device__ uint32_t compat_lane(Ctx& t, uint32_t w) {
+    const int s = side_of(t.g, w);
+    if (t.nss[1 - s] == 0) return 0;
+    uint32_t miss = 0;
+    for (uint32_t i = 0; i < t.ns; ++i) {
+        const uint32_t m = t.sid[i];
+        if (side_of(t.g, m) == s) continue;
+        if (adj_test(t, w, m)) continue;
+        if (++miss > t.k || t.smc[i] >= t.k) return t.k + 1;
+    }
+    return miss;
+}
+
+// Adds c to S (warp); returns its misses.  The members that reach k misses
+// because of c go to t.sat (first kSatCap, in S order), their count to *nsat.
+__device__ uint32_t push_member(Ctx& t, uint32_t c, uint32_t* nsat_out) {
+    const int s = side_of(t.g, c);
+    uint32_t miss = 0, nsat = 0;
+    for (uint32_t base = 0; base < t.ns; base += 32) {
+        const uint32_t i = base + t.lane;
+        bool nm = false, sat = false;
+        uint32_t m = 0;
+        if (i < t.ns) {
+            m = t.sid[i];
+            if (side_of(t.g, m) != s && !adj_test(t, c, m)) {
+                nm = true;
+                const uint32_t v = t.smc[i] + 1;
+                t.smc[i] = v;
+                sat = v == t.k;
+            }
+        }
+        miss += __popc(__ballot_sync(kFull, nm));
+        const uint32_t sm = __ballot_sync(kFull, sat);
+        if (sat) {
+            const uint32_t r = nsat + __popc(sm & lanemask_lt());
+            if (r < kSatCap) t.sat[r] = m;
+        }
+        nsat += __popc(sm);
+    }
+    if (t.lane == 0) {
+        t.sid[t.ns] = c;
+        t.smc[t.ns] = miss;
+    }
+    __syncwarp();
+    t.ns++;
+    t.nss[s]++;
+    if (nsat_out) *nsat_out = nsat < kSatCap ? nsat : kSatCap;
+    return miss;
+}
+
+__device__ void pop_member(Ctx& t) {
+    const uint32_t c = t.sid[t.ns - 1];
+    t.ns--;
+    const int s = side_of(t.g, c);
+    t.nss[s]--;
+    for (uint32_t base = 0; base < t.ns; base += 32) {
+        const uint32_t i = base + t.lane;
+        if (i < t.ns) {
+            const uint32_t m = t.sid[i];
+            if (side_of(t.g, m) != s && !adj_test(t, c, m)) t.smc[i]--;
+        }
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ void pop_to(Ctx& t, uint32_t ns) {
+    while (t.ns > ns) pop_member(t);
+}
+
+// The first `want` members of side `s` in S order into dst (warp); returns
+// how many were found.
+__device__ uint32_t first_members(Ctx& t, int s, uint32_t want, uint32_t* dst) {
+    uint32_t got = 0;
+    for (uint32_t base = 0; base < t.ns && got < want; base += 32) {
+        const uint32_t i = base + t.lane;
+        const bool on = i < t.ns && side_of(t.g, t.sid[i]) == s;
+        const uint32_t mask = __ballot_sync(kFull, on);
+        if (on) {
+            const uint32_t r = got + __popc(mask & lanemask_lt());
+            if (r < want) dst[r] = t.sid[i];
+        }
+        got += __popc(mask);
+    }
+    __syncwarp();
+    return got < want ? got : want;
+}
+
+// ----------------------------------------------------------------- leaf / prune tests
+
+// Warp form of outsider_addable (enum_core.cuh): both candidate sides local.
+__device__ bool outsider_addable(Ctx& t, const uint32_t* l0, uint32_t n0, const uint32_t* l1,
+                                 uint32_t n1, const uint32_t* tot) {
+    const GraphView& g = t.g;
+    for (int s = 0; s < 2; ++s) {
+        const int o = 1 - s;
+        const uint32_t* ls = s ? l1 : l0;
+        const uint32_t* lo = s ? l0 : l1;
+        const uint32_t cs = s ? n1 : n0, co = s ? n0 : n1;
+        const uint32_t* tots_o = tot + t.ns + (o ? n0 : 0);
+        const uint32_t nopp = t.nss[o] + co, nown = t.nss[s] + cs;
+        // the lowest-degree blocking member (tot >= k), S members first
+        unsigned long long best = ~0ull;
+        for (uint32_t base = 0; base < t.ns; base += 32) {
+            const uint32_t i = base + t.lane;
+            if (i < t.ns) {
+                const uint32_t m = t.sid[i];
+                if (side_of(g, m) == o && tot[i] >= t.k) {
+                    const unsigned long long key = ((unsigned long long)degree(g, m) << 32) | i;
+                    best = key < best ? key : best;
+                }
+            }
+        }
+        for (uint32_t base = 0; base < co; base += 32) {
+            const uint32_t q = base + t.lane;
+            if (q < co && tots_o[q] >= t.k) {
+                const unsigned long long key =
+                    ((unsigned long long)degree(g, lo[2 * q]) << 32) | (t.ns + q);
+                best = key < best ? key : best;
+            }
+        }
+        best = warp_min64(best);
+        uint32_t nsrc = 0;
+        if (best != ~0ull) {
+            const uint32_t pos = (uint32_t)best;
+            if (t.lane == 0) t.src[0] = pos < t.ns ? t.sid[pos] : lo[2 * (pos - t.ns)];
+            __syncwarp();
+            nsrc = 1;
+        } else if (nopp >= t.k + 1) {
+            nsrc = first_members(t, o, t.k + 1, t.src);
+            if (nsrc < t.k + 1) {
+                for (uint32_t q = t.lane; q + nsrc < t.k + 1 && q < co; q += 32)
+                    t.src[nsrc + q] = lo[2 * q];
+                __syncwarp();
+                const uint32_t more = t.k + 1 - nsrc;
+                nsrc += more < co ? more : co;
+            }
+        } else {
+            if (side_end(g, s) - side_begin(g, s) > nown) return true;
+            continue;
+        }
+        for (uint32_t q = 0; q < nsrc; ++q) {
+            const uint32_t m = t.src[q];
+            const uint32_t d = degree(g, m);
+            const uint32_t* row = g.adj + g.off[m];
+            if (t.lane == 0) t.work += d;
+            for (uint32_t base = 0; base < d; base += 32) {
+                const uint32_t p = base + t.lane;
+                bool ok = false;
+                if (p < d) {
+                    const uint32_t e = row[p];
+                    bool skip = false;
+                    for (uint32_t r = 0; r < q && !skip; ++r) skip = adj_test(t, e, t.src[r]);
+                    for (uint32_t i = 0; i < t.ns && !skip; ++i) skip = t.sid[i] == e;
+                    for (uint32_t i = 0; i < cs && !skip; ++i) skip = ls[2 * i] == e;
+                    if (!skip) {
+                        uint32_t miss = 0;
+                        ok = true;
+                        for (uint32_t i = 0; i < t.ns && ok; ++i) {
+                            const uint32_t w = t.sid[i];
+                            if (side_of(g, w) != o || adj_test(t, e, w)) continue;
+                            if (++miss > t.k || tot[i] >= t.k) ok = false;
+                        }
+                        for (uint32_t i = 0; i < co && ok; ++i) {
+                            if (adj_test(t, e, lo[2 * i])) continue;
+                            if (++miss > t.k || tots_o[i] >= t.k) ok = false;
+                        }
+                    }
+                }
+                if (__any_sync(kFull, ok)) return true;
+            }
+        }
+    }
+    return false;
+}
+
+// Warp form of outsider_addable_mixed (enum_core.cuh): side s global (ids >
+// lo), side o local (list l, n entries).  Scratch at `tot`: n list totals,
+// then the S_o member ids and their totals (2 ns words).
+__device__ bool outsider_addable_mixed(Ctx& t, int s, uint32_t lo, const uint32_t* l, uint32_t n,
+                                       uint32_t* tot) {
+    const GraphView& g = t.g;
+    const int o = 1 - s;
+    const uint32_t G = side_end(g, s) - lo - 1;
+    uint32_t* mem = tot + n;
+    uint32_t* memtot = mem + t.ns;
+    uint32_t nm = 0;
+    unsigned long long best = ~0ull;
+    for (uint32_t base = 0; base < t.ns; base += 32) {
+        const uint32_t i = base + t.lane;
+        const bool on = i < t.ns && side_of(g, t.sid[i]) == o;
+        const uint32_t mask = __ballot_sync(kFull, on);
+        if (on) {
+            const uint32_t w = t.sid[i];
+            const uint32_t r = nm + __popc(mask & lanemask_lt());
+            const uint32_t tw = t.smc[i] + G - count_above(g, w, lo, &t.work);
+            mem[r] = w;
+            memtot[r] = tw;
+            if (tw >= t.k) {
+                const unsigned long long key = ((unsigned long long)degree(g, w) << 32) | i;
+                best = key < best ? key : best;
+            }
+        }
+        nm += __popc(mask);
+    }
+    for (uint32_t base = 0; base < n; base += 32) {
+        const uint32_t q = base + t.lane;
+        if (q < n) {
+            const uint32_t w = l[2 * q];
+            const uint32_t tq = l[2 * q + 1] + G - count_above(g, w, lo, &t.work);
+            tot[q] = tq;
+            if (tq >= t.k) {
+                const unsigned long long key = ((unsigned long long)degree(g, w) << 32) | (t.ns + q);
+                best = key < best ? key : best;
+            }
+        }
+    }
+    best = warp_min64(best);
+    __syncwarp();
+    const uint32_t nopp = nm + n;
+    uint32_t nsrc = 0;
+    if (best != ~0ull) {
+        const uint32_t pos = (uint32_t)best;
+        if (t.lane == 0) t.src[0] = pos < t.ns ? t.sid[pos] : l[2 * (pos - t.ns)];
+        nsrc = 1;
+    } else if (nopp >= t.k + 1) {
+        for (uint32_t j = t.lane; j < t.k + 1; j += 32) t.src[j] = j < nm ? mem[j] : l[2 * (j - nm)];
+        nsrc = t.k + 1;
+    } else {
+        return (lo + 1 - side_begin(g, s)) > t.nss[s];
+    }
+    __syncwarp();
+    for (uint32_t q = 0; q < nsrc; ++q) {
+        const uint32_t m = t.src[q];
+        const uint32_t d = degree(g, m);
+        const uint32_t* row = g.adj + g.off[m];
+        if (t.lane == 0) t.work += d;
+        for (uint32_t base = 0; base < d; base += 32) {
+            const uint32_t p = base + t.lane;
+            bool ok = false, past = false;
+            if (p < d) {
+                const uint32_t e = row[p];
+                past = e > lo;                  // rows are sorted: the rest is in C
+                if (!past) {
+                    bool skip = false;
+                    for (uint32_t r = 0; r < q && !skip; ++r) skip = adj_test(t, e, t.src[r]);
+                    for (uint32_t i = 0; i < t.ns && !skip; ++i) skip = t.sid[i] == e;
+                    if (!skip) {
+                        uint32_t miss = 0;
+                        ok = true;
+                        for (uint32_t i = 0; i < nm && ok; ++i) {
+                            if (adj_test(t, e, mem[i])) continue;
+                            if (++miss > t.k || memtot[i] >= t.k) ok = false;
+                        }
+                        for (uint32_t r = 0; r < n && ok; ++r) {
+                            if (adj_test(t, e, l[2 * r])) continue;
+                            if (++miss > t.k || tot[r] >= t.k) ok = false;
+                        }
+                    }
+                }
+            }
+            if (__any_sync(kFull, ok)) return true;
+            if (__any_sync(kFull, past)) break;
+        }
+    }
+    return false;
+}
+
+// ----------------------------------------------------------------- emission
+
+__device__ void emit(Ctx& t, const Outputs& o, const uint32_t* l0, uint32_t n0, const uint32_t* l1,
+                     uint32_t n1) {
+    unsigned long long a = 0, b = 0;
+    for (uint32_t i = t.lane; i < t.ns; i += 32) {
+        const unsigned long long e = elem_a(t.sid[i]);
+        a += e; b += elem_b(e);
+    }
+    for (uint32_t i = t.lane; i < n0; i += 32) {
+        const unsigned long long e = elem_a(l0[2 * i]);
+        a += e; b += elem_b(e);
+    }
+    for (uint32_t i = t.lane; i < n1; i += 32) {
+        const unsigned long long e = elem_a(l1[2 * i]);
+        a += e; b += elem_b(e);
+    }
+    a = warp_sum64(a);
+    b = warp_sum64(b);
+    const uint32_t nx = t.nss[0] + n0, ny = t.nss[1] + n1;
+    if (o.out_buf) {
+        // record mode: one reservation per result, exact limit
+        const unsigned long long words = 2ull + nx + ny;
+        unsigned long long c = 0, at = 0;
+        if (t.lane == 0) {
+            c = atomicAdd(o.count, 1ull);
+            if (!(o.limit && c >= o.limit)) {
+                if (o.limit && c + 1 >= o.limit) atomicExch(o.stop, 1);
+                atomicAdd(o.hash_sum, final_h1(a, nx, ny));
+                atomicXor(o.hash_xor, final_h2(b, nx, ny));
+                at = atomicAdd(o.out_pos, words);
+            } else {
+                atomicExch(o.stop, 1);
+            }
+        }
+        c = bcast(c);
+        at = bcast(at);
+        if (o.limit && c >= o.limit) return;
+        if (at + words > o.out_cap) return;   // the host sees out_pos > cap: overflow
+        uint32_t* r = o.out_buf + at;
+        if (t.lane == 0) { r[0] = nx; r[1] = ny; }
+        uint32_t px = 2, py = 2 + nx;
+        for (uint32_t base = 0; base < t.ns; base += 32) {
+            const uint32_t i = base + t.lane;
+            const bool in = i < t.ns;
+            const uint32_t v = in ? t.sid[i] : 0;
+            const bool isy = in && side_of(t.g, v);
+            const uint32_t my = __ballot_sync(kFull, isy);
+            const uint32_t mx = __ballot_sync(kFull, in && !isy);
+            if (isy) r[py + __popc(my & lanemask_lt())] = v;
+            else if (in) r[px + __popc(mx & lanemask_lt())] = v;
+            px += __popc(mx);
+            py += __popc(my);
+        }
+        for (uint32_t i = t.lane; i < n0; i += 32) r[px + i] = l0[2 * i];
+        for (uint32_t i = t.lane; i < n1; i += 32) r[py + i] = l1[2 * i];
+        return;
+    }
+    t.cnt++;
+    t.hsum += final_h1(a, nx, ny);
+    t.hxor ^= final_h2(b, nx, ny);
+    if (t.cnt >= kFlushBatch) flush(t, o);
+}
+
+// ----------------------------------------------------------------- frames
+
+struct Hdr {
+    uint32_t ns, flags, lo[2], cnt[2], off[2], order, phase, pos, top, parent, end;
+};
+
+__device__ __forceinline__ Hdr read_hdr(const uint32_t* f) {
+    Hdr h;
+    h.ns = f[F_NS]; h.flags = f[F_FLAGS];
+    h.lo[0] = f[F_LO0]; h.lo[1] = f[F_LO1];
+    h.cnt[0] = f[F_CNT0]; h.cnt[1] = f[F_CNT1];
+    h.off[0] = f[F_OFF0]; h.off[1] = f[F_OFF1];
+    h.order = f[F_ORDER]; h.phase = f[F_PHASE]; h.pos = f[F_POS];
+    h.top = f[F_TOP]; h.parent = f[F_PARENT_SLOT]; h.end = f[F_END];
+    return h;
+}
+
+__device__ __forceinline__ void write_hdr(uint32_t* f, const Hdr& h) {
+    f[F_NS] = h.ns; f[F_FLAGS] = h.flags;
+    f[F_LO0] = h.lo[0]; f[F_LO1] = h.lo[1];
+    f[F_CNT0] = h.cnt[0]; f[F_CNT1] = h.cnt[1];
+    f[F_OFF0] = h.off[0]; f[F_OFF1] = h.off[1];
+    f[F_ORDER] = h.order; f[F_PHASE] = h.phase; f[F_POS] = h.pos;
+    f[F_TOP] = h.top; f[F_PARENT_SLOT] = h.parent; f[F_END] = h.end;
+}
+
+__device__ __forceinline__ void set_word(Ctx& t, uint32_t at, uint32_t v) {
+    if (t.lane == 0) t.arena[at] = v;
+    __syncwarp();
+}
+
+// Appends the lanes' kept (v, m) pairs at arena[w + 2 cnt], in lane order.
+__device__ __forceinline__ void append_pair(Ctx& t, uint32_t w, uint32_t& cnt, bool keep,
+                                            uint32_t v, uint32_t m) {
+    const uint32_t mask = __ballot_sync(kFull, keep);
+    if (keep) {
+        const uint32_t r = cnt + __popc(mask & lanemask_lt());
+        t.arena[w + 2 * r] = v;
+        t.arena[w + 2 * r + 1] = m;
+    }
+    cnt += __popc(mask);
+}
+
+// Warp form of build_child (enum_core.cuh): the child "S + c" of frame cur.
+__device__ uint32_t build_child(Ctx& t, const Outputs& o, uint32_t cur, uint32_t c, int s,
+                                uint32_t p, bool forced, bool opp_done) {
+    const GraphView& g = t.g;
+    const Hdr f = read_hdr(t.arena + cur);
+    pop_to(t, f.ns);
+    if (t.ns + 1 > t.smax) { fail(t, o, TASK_E_SMAX); return kNoPos; }
+    uint32_t nsat = 0;
+    const uint32_t mcc = push_member(t, c, &nsat);
+    const int os = 1 - s;
+    const uint32_t nc = f.top;
+    uint32_t w = nc + F_WORDS;
+    if (w > t.cap) { fail(t, o, TASK_E_ARENA); return kNoPos; }
+    Hdr ch;
+    ch.ns = t.ns; ch.flags = 0; ch.lo[0] = ch.lo[1] = 0; ch.cnt[0] = ch.cnt[1] = 0;
+    ch.order = 0; ch.phase = 0; ch.pos = 0; ch.parent = cur; ch.end = 0xFFFFFFFFu;
+
+    // ---- same side as c
+    ch.off[s] = w;
+    uint32_t cnt = 0;
+    if (f.flags & gbit(s)) {
+        if (nsat == 0) {
+            ch.flags |= gbit(s);
+            ch.lo[s] = c;
+        } else {
+            uint32_t z = t.sat[0];
+            for (uint32_t i = 1; i < nsat; ++i)
+                if (degree(g, t.sat[i]) < degree(g, z)) z = t.sat[i];
+            const uint32_t dz = degree(g, z);
+            if (w + 2ull * dz > t.cap) { fail(t, o, TASK_E_ARENA); return kNoPos; }
+            if (t.lane == 0) t.work += dz;
+            const uint32_t* row = g.adj + g.off[z];
+            for (uint32_t base = 0; base < dz; base += 32) {
+                const uint32_t q = base + t.lane;
+                bool keep = false;
+                uint32_t v = 0, m = 0;
+                if (q < dz) {
+                    v = row[q];
+                    if (v > c) {
+                        m = compat_lane(t, v);
+                        keep = m <= t.k;
+                    }
+                }
+                append_pair(t, w, cnt, keep, v, m);
+            }
+        }
+    } else {
+        const uint32_t* lst = t.arena + f.off[s];
+        const uint32_t n = f.cnt[s];
+        if (w + 2ull * n > t.cap) { fail(t, o, TASK_E_ARENA); return kNoPos; }
+        const uint32_t start = forced ? 0u : p + 1;
+        for (uint32_t base = start; base < n; base += 32) {
+            const uint32_t q = base + t.lane;
+            bool keep = false;
+            uint32_t v = 0, m = 0;
+            if (q < n && q != p) {
+                v = lst[2 * q];
+                m = lst[2 * q + 1];
+                keep = true;
+                for (uint32_t i = 0; i < nsat && keep; ++i) keep = adj_test(t, v, t.sat[i]);
+            }
+            append_pair(t, w, cnt, keep, v, m);
+        }
+    }
+    ch.cnt[s] = cnt;
+    w += 2 * cnt;
+
+    // ---- other side
+    ch.off[os] = w;
+    cnt = 0;
+    if (opp_done) {
+        // that side was iterated first: nothing left on it
+    } else if (f.flags & gbit(os)) {
+        const uint32_t lo = f.lo[os];
+        if (t.nss[s] <= t.k && mcc < t.k) {
+            ch.flags |= gbit(os);
+            ch.lo[os] = lo;
+        } else {
+            // candidates touch c (saturated) or one of k+1 members of side s
+            uint32_t nsrc;
+            if (mcc >= t.k) {
+                if (t.lane == 0) t.src[0] = c;
+                __syncwarp();
+                nsrc = 1;
+            } else {
+                nsrc = first_members(t, s, t.k + 1, t.src);
+            }
+            unsigned long long bound = 0;
+            for (uint32_t q = 0; q < nsrc; ++q) bound += degree(g, t.src[q]);
+            if (w + 2 * bound > t.cap) { fail(t, o, TASK_E_ARENA); return kNoPos; }
+            for (uint32_t q = 0; q < nsrc; ++q) {
+                const uint32_t m = t.src[q];
+                const uint32_t d = degree(g, m);
+                const uint32_t* row = g.adj + g.off[m];
+                if (t.lane == 0) t.work += d;
+                for (uint32_t base = 0; base < d; base += 32) {
+                    const uint32_t e = base + t.lane;
+                    bool keep = false;
+                    uint32_t v = 0, mm = 0;
+                    if (e < d) {
+                        v = row[e];
+                        if (v > lo) {
+                            bool seen = false;
+                            for (uint32_t r = 0; r < q && !seen; ++r) seen = adj_test(t, v, t.src[r]);
+                            if (!seen) {
+                                mm = compat_lane(t, v);
+                                keep = mm <= t.k;
+                            }
+                        }
+                    }
+                    append_pair(t, w, cnt, keep, v, mm);
+                }
+            }
+        }
+    } else {
+        const uint32_t* lst = t.arena + f.off[os];
+        const uint32_t n = f.cnt[os];
+        if (w + 2ull * n > t.cap) { fail(t, o, TASK_E_ARENA); return kNoPos; }
+        for (uint32_t base = 0; base < n; base += 32) {
+            const uint32_t q = base + t.lane;
+            bool keep = false;
+            uint32_t v = 0, m = 0;
+            if (q < n) {
+                v = lst[2 * q];
+                const uint32_t cm = lst[2 * q + 1];
+                const bool a = adj_test(t, v, c);
+                keep = a || (cm + 1 <= t.k && mcc < t.k);
+                m = cm + (a ? 0u : 1u);
+            }
+            append_pair(t, w, cnt, keep, v, m);
+        }
+    }
+    ch.cnt[os] = cnt;
+    w += 2 * cnt;
+    ch.top = w;
+    for (int s2 = 0; s2 < 2; ++s2)
+        if ((ch.flags & gbit(s2)) && ch.lo[s2] + 1 >= side_end(g, s2)) {
+            ch.flags &= ~gbit(s2);
+            ch.cnt[s2] = 0;
+        }
+    if (t.lane == 0) write_hdr(t.arena + nc, ch);
+    __syncwarp();
+    return nc;
+}
+
+// Warp form of enter_node (enum_core.cuh).
+__device__ int enter_node(Ctx& t, const Outputs& o, uint32_t cur, uint32_t* next) {
+    const GraphView& g = t.g;
+    const Hdr f = read_hdr(t.arena + cur);
+    pop_to(t, f.ns);
+    const bool g0 = f.flags & FL_G0, g1 = f.flags & FL_G1;
+    if (t.nss[1] == 0 && !g1 && f.cnt[1] == 0) return ENTER_DONE;   // Y must end up non-empty
+    if (g0 != g1) {
+        const int s = g0 ? 0 : 1, os = 1 - s;
+        const uint32_t n = f.cnt[os];
+        const uint32_t base = f.top;
+        if (base + n + 2ull * t.ns > t.cap) { fail(t, o, TASK_E_ARENA); return ENTER_DONE; }
+        if (outsider_addable_mixed(t, s, f.lo[s], t.arena + f.off[os], n, t.arena + base))
+            return ENTER_DONE;
+    }
+    if (!g0 && !g1) {
+        const uint32_t n0 = f.cnt[0], n1 = f.cnt[1];
+        const uint32_t* l0 = t.arena + f.off[0];
+        const uint32_t* l1 = t.arena + f.off[1];
+        const unsigned long long pairs = (unsigned long long)(t.ns + n0) * (t.ns + n1);
+        if (n0 + n1 == 0 || pairs <= t.scan_limit) {
+            const uint32_t base = f.top;
+            if (base + (unsigned long long)t.ns + n0 + n1 > t.cap) {
+                fail(t, o, TASK_E_ARENA);
+                return ENTER_DONE;
+            }
+            uint32_t* tot = t.arena + base;
+            uint32_t* tot0 = tot + t.ns;
+            uint32_t* tot1 = tot0 + n0;
+            // misses inside S u C
+            for (uint32_t i = t.lane; i < t.ns; i += 32) {
+                const uint32_t v = t.sid[i];
+                const int sv = side_of(g, v);
+                const uint32_t* lo = sv ? l0 : l1;
+                const uint32_t no = sv ? n0 : n1;
+                uint32_t m = t.smc[i];
+                for (uint32_t q = 0; q < no; ++q) m += adj_test(t, v, lo[2 * q]) ? 0u : 1u;
+                tot[i] = m;
+            }
+            for (uint32_t q = t.lane; q < n1; q += 32) tot1[q] = l1[2 * q + 1];
+            __syncwarp();
+            for (uint32_t abase = 0; abase < n0; abase += 32) {
+                const uint32_t a = abase + t.lane;
+                const uint32_t va = a < n0 ? l0[2 * a] : 0u;
+                uint32_t ta = a < n0 ? l0[2 * a + 1] : 0u;
+                for (uint32_t b = 0; b < n1; ++b) {
+                    const bool miss = a < n0 && !adj_test(t, va, l1[2 * b]);
+                    ta += miss ? 1u : 0u;
+                    const uint32_t mb = __popc(__ballot_sync(kFull, miss));
+                    if (t.lane == 0 && mb) tot1[b] += mb;
+                }
+                if (a < n0) tot0[a] = ta;
+            }
+            __syncwarp();
+            bool bad = false;
+            for (uint32_t i = t.lane; i < t.ns + n0 + n1; i += 32) bad |= tot[i] > t.k;
+            if (!__any_sync(kFull, bad)) {
+                // S u C is a k-biplex: the only leaf that can be maximal
+                if (!outsider_addable(t, l0, n0, l1, n1, tot)) emit(t, o, l0, n0, l1, n1);
+                return ENTER_DONE;
+            }
+            if (outsider_addable(t, l0, n0, l1, n1, tot)) return ENTER_DONE;
+            // forced candidate: fits every leaf that lacks it (first in list order)
+            for (int s = 0; s < 2; ++s) {
+                const uint32_t* ls = s ? l1 : l0;
+                const uint32_t* ts = s ? tot1 : tot0;
+                const uint32_t cs = s ? n1 : n0;
+                const uint32_t* lo = s ? l0 : l1;
+                const uint32_t* to = s ? tot0 : tot1;
+                const uint32_t co = s ? n0 : n1;
+                for (uint32_t qbase = 0; qbase < cs; qbase += 32) {
+                    const uint32_t q = qbase + t.lane;
+                    bool ok = false;
+                    if (q < cs && ts[q] <= t.k) {
+                        const uint32_t c = ls[2 * q];
+                        ok = true;
+                        for (uint32_t i = 0; i < t.ns && ok; ++i) {
+                            const uint32_t v = t.sid[i];
+                            if (side_of(g, v) == s || adj_test(t, c, v)) continue;
+                            ok = tot[i] <= t.k;
+                        }
+                        for (uint32_t r = 0; r < co && ok; ++r)
+                            if (!adj_test(t, c, lo[2 * r])) ok = to[r] <= t.k;
+                    }
+                    const uint32_t mask = __ballot_sync(kFull, ok);
+                    if (mask) {
+                        const uint32_t qq = qbase + __ffs(mask) - 1;
+                        const uint32_t c = ls[2 * qq];
+                        const uint32_t chn = build_child(t, o, cur, c, s, qq, true, false);
+                        if (chn == kNoPos) return ENTER_DONE;
+                        *next = chn;
+                        return ENTER_PUSHED;
+                    }
+                }
+            }
+        }
+    }
+    // iterate: local sides before global ones; between two local sides the shorter first
+    uint32_t order;
+    if (f.flags & FL_ROOT) order = 1u;   // the root branches on V first; root chunks rely on it
+    else if (g0 != g1) order = g0 ? 1u : 0u;
+    else if (!g0) order = GMK_LOCAL_ORDER(f.cnt[0], f.cnt[1]);
+    else order = 1u;
+    if (t.lane == 0) {
+        uint32_t* fw = t.arena + cur;
+        fw[F_ORDER] = order;
+        fw[F_PHASE] = 0;
+        fw[F_POS] = (f.flags & gbit((int)order)) ? f.lo[order] + 1 : 0;
+    }
+    __syncwarp();
+    return ENTER_ITERATE;
+}
+
+// Warp form of next_child (enum_core.cuh).
+__device__ uint32_t next_child(Ctx& t, const Outputs& o, uint32_t cur) {
+    const GraphView& g = t.g;
+    uint32_t* f = t.arena + cur;
+    const Hdr h = read_hdr(f);
+    uint32_t phase = h.phase, pos = h.pos;
+    while (phase < 2) {
+        const int s = phase == 0 ? (int)h.order : 1 - (int)h.order;
+        const bool opp_done = phase == 1;
+        uint32_t c = 0, p = kNoPos;
+        bool have = false;
+        if (h.flags & gbit(s)) {
+            const uint32_t end = phase == 0 && h.end < side_end(g, s) ? h.end : side_end(g, s);
+            if (pos < end) { c = pos; p = kNoPos; ++pos; have = true; }
+        } else if (pos < h.cnt[s]) {
+            p = pos;
+            c = t.arena[h.off[s] + 2 * p];
+            ++pos;
+            have = true;
+        }
+        // U children after the V side is exhausted need a V member in S
+        if (have && opp_done && s == 0) {
+            bool anyv = false;
+            for (uint32_t i = t.lane; i < h.ns; i += 32) anyv |= side_of(g, t.sid[i]) != 0;
+            if (!__any_sync(kFull, anyv)) { have = false; phase = 2; }
+        }
+        if (!have) {
+            if (phase == 2) break;
+            ++phase;
+            if (phase == 1) {
+                const int s2 = 1 - (int)h.order;
+                pos = (h.flags & gbit(s2)) ? h.lo[s2] + 1 : 0;
+            }
+            continue;
+        }
+        if (t.lane == 0) { f[F_PHASE] = phase; f[F_POS] = pos; }
+        __syncwarp();
+        return build_child(t, o, cur, c, s, p, false, opp_done);
+    }
+    if (t.lane == 0) { f[F_PHASE] = phase; f[F_POS] = pos; }
+    __syncwarp();
+    return kNoPos;
+}
+
+// ----------------------------------------------------------------- splitting
+
+// Does frame x still have children to explore (or, for the current frame,
+// anything to do)?
+__device__ __forceinline__ bool frame_pending(const uint32_t* f, bool is_cur) {
+    if (!(f[F_FLAGS] & FL_ENTERED)) return is_cur;
+    return f[F_PHASE] < 2;
+}
+
+__device__ __forceinline__ uint32_t frame_list_words(const uint32_t* f) {
+    const uint32_t c0 = (f[F_FLAGS] & FL_G0) ? 0u : f[F_CNT0];
+    const uint32_t c1 = (f[F_FLAGS] & FL_G1) ? 0u : f[F_CNT1];
+    return 2 * (c0 + c1);
+}
+
+// Bounded CAS reservation of `want` units under `cap`; returns the start or
+// ~0ull when it does not fit.
+__device__ unsigned long long reserve(unsigned long long* ctr, unsigned long long want,
+                                      unsigned long long cap) {
+    unsigned long long cur = *(volatile unsigned long long*)ctr;
+    for (int tries = 0; tries < 64; ++tries) {
+        if (cur + want > cap) return ~0ull;
+        const unsigned long long prev = atomicCAS(ctr, cur, cur + want);
+        if (prev == cur) return cur;
+        cur = prev;
+    }
+    return ~0ull;
+}
+
+// Writes every pending frame on the path from `cur` to the root as a task of
+// the next round.  All-or-nothing: returns false (and writes nothing) when
+// the buffer cannot take them all.
+__device__ bool split_path(Ctx& t, const SplitBuf& sb, uint32_t cur) {
+    // sizes first
+    unsigned long long words = 0, recs = 0;
+    for (uint32_t x = cur; x != kNoPos; x = t.arena[x + F_PARENT_SLOT]) {
+        const uint32_t* f = t.arena + x;
+        if (!frame_pending(f, x == cur)) continue;
+        if ((f[F_FLAGS] & FL_ROOT) && !(f[F_FLAGS] & FL_ENTERED)) return false;
+        words += 3ull + 2ull * f[F_NS] + F_WORDS + frame_list_words(f);
+        ++recs;
+    }
+    if (recs == 0) return false;
+    unsigned long long w0 = 0, r0 = 0;
+    if (t.lane == 0) {
+        w0 = reserve(sb.used, words, sb.word_cap);
+        r0 = w0 == ~0ull ? ~0ull : reserve(sb.count, recs, sb.idx_cap);
+    }
+    w0 = bcast(w0);
+    r0 = bcast(r0);
+    if (w0 == ~0ull || r0 == ~0ull) return false;   // a failed word reservation is left unused
+    unsigned long long wp = w0, rp = r0;
+    for (uint32_t x = cur; x != kNoPos; x = t.arena[x + F_PARENT_SLOT]) {
+        const uint32_t* f = t.arena + x;
+        if (!frame_pending(f, x == cur)) continue;
+        pop_to(t, f[F_NS]);
+        const uint32_t ns = f[F_NS];
+        const uint32_t c0 = (f[F_FLAGS] & FL_G0) ? 0u : f[F_CNT0];
+        const uint32_t c1 = (f[F_FLAGS] & FL_G1) ? 0u : f[F_CNT1];
+        uint32_t* r = sb.words + wp;
+        if (t.lane == 0) { r[0] = ns; r[1] = c0; r[2] = c1; sb.idx[rp] = wp; }
+        for (uint32_t i = t.lane; i < ns; i += 32) { r[3 + i] = t.sid[i]; r[3 + ns + i] = t.smc[i]; }
+        uint32_t* fr = r + 3 + 2 * ns;
+        if (t.lane < F_WORDS) fr[t.lane] = f[t.lane];
+        uint32_t* lr = fr + F_WORDS;
+        const uint32_t* a0 = t.arena + f[F_OFF0];
+        const uint32_t* a1 = t.arena + f[F_OFF1];
+        for (uint32_t i = t.lane; i < 2 * c0; i += 32) lr[i] = a0[i];
+        for (uint32_t i = t.lane; i < 2 * c1; i += 32) lr[2 * c0 + i] = a1[i];
+        wp += 3ull + 2ull * ns + F_WORDS + 2ull * (c0 + c1);
+        ++rp;
+    }
+    __syncwarp();
+    return true;
+}
+
+// ----------------------------------------------------------------- tasks
+
+struct RunLimits {
+    uint32_t split_min_nodes;           // 0: never split
+    const unsigned long long* queue;    // the round's queue head
+    unsigned long long queue_len;       // entries this warp's round hands out
+};
+
+// Depth-first search from the frame at arena offset 0.
+__device__ void run_dfs(Ctx& t, const Outputs& o, uint32_t first, const SplitBuf* sb,
+                        const RunLimits& lim) {
+    uint32_t cur = 0;
+    uint32_t polls = 0;
+    unsigned long long task_nodes = 0;
+    bool may_split = lim.split_min_nodes != 0 && sb != nullptr;
+    while (cur != kNoPos) {
+        if (t.err) break;
+        if ((++polls & 63u) == 0) {
+            int stop = 0, late = 0, hungry = 0;
+            if (t.lane == 0) {
+                stop = load_flag(o.stop);
+                late = o.deadline_ns && now_ns() > o.deadline_ns;
+                hungry = may_split && task_nodes >= lim.split_min_nodes &&
+                         *(volatile const unsigned long long*)lim.queue >= lim.queue_len;
+            }
+            stop = bcast(stop); late = bcast(late); hungry = bcast(hungry);
+            if (stop) break;
+            if (late) { fail(t, o, TASK_E_TIMEOUT); break; }
+            if (hungry) {
+                if (split_path(t, *sb, cur)) break;
+                may_split = false;   // buffer full: finish this task here
+            }
+        }
+        uint32_t* f = t.arena + cur;
+        const uint32_t flags = f[F_FLAGS];
+        if (!(flags & FL_ENTERED)) {
+            if (t.lane == 0) f[F_FLAGS] = flags | FL_ENTERED;
+            __syncwarp();
+            t.nodes++;
+            task_nodes++;
+            uint32_t nxt = kNoPos;
+            const int r = enter_node(t, o, cur, &nxt);
+            if (r == ENTER_PUSHED) { set_word(t, cur + F_PHASE, 2); cur = nxt; continue; }
+            if (r == ENTER_DONE) { set_word(t, cur + F_PHASE, 2); cur = f[F_PARENT_SLOT]; continue; }
+            if ((flags & FL_ROOT) && f[F_ORDER] == 1u && (f[F_FLAGS] & FL_G1)) {
+                const uint32_t p = f[F_POS];
+                set_word(t, cur + F_POS, first > p ? first : p);
+            }
+        }
+        const uint32_t ch = next_child(t, o, cur);
+        if (ch == kNoPos) { cur = f[F_PARENT_SLOT]; continue; }
+        cur = ch;
+    }
+    pop_to(t, 0);
+}
+
+// Root task: x in U with its first-level children y in [first, last).
+__device__ void run_root(Ctx& t, const Outputs& o, uint32_t root, uint32_t first, uint32_t last,
+                         const SplitBuf* sb, const RunLimits& lim) {
+    t.ns = 0; t.nss[0] = t.nss[1] = 0;
+    push_member(t, root, nullptr);
+    Hdr h;
+    h.ns = 1; h.flags = FL_G0 | FL_G1 | FL_ROOT;
+    h.lo[0] = root; h.lo[1] = t.g.nl - 1;
+    h.cnt[0] = h.cnt[1] = 0;
+    h.off[0] = h.off[1] = F_WORDS;
+    h.order = 0; h.phase = 0; h.pos = 0;
+    h.top = F_WORDS; h.parent = kNoPos; h.end = last;
+    for (int s = 0; s < 2; ++s)
+        if ((h.flags & gbit(s)) && h.lo[s] + 1 >= side_end(t.g, s)) {
+            h.flags &= ~gbit(s);
+            h.cnt[s] = 0;
+        }
+    if (t.lane == 0) write_hdr(t.arena, h);
+    __syncwarp();
+    run_dfs(t, o, first, sb, lim);
+}
+
+// Resumed task: a frame written by split_path.
+__device__ void run_record(Ctx& t, const Outputs& o, const uint32_t* r, const SplitBuf* sb,
+                           const RunLimits& lim) {
+    const uint32_t ns = r[0], c0 = r[1], c1 = r[2];
+    if (ns > t.smax) { fail(t, o, TASK_E_SMAX); return; }
+    if (F_WORDS + 2ull * (c0 + c1) > t.cap) { fail(t, o, TASK_E_ARENA); return; }
+    uint32_t nv = 0;
+    for (uint32_t base = 0; base < ns; base += 32) {
+        const uint32_t i = base + t.lane;
+        bool isv = false;
+        if (i < ns) {
+            const uint32_t v = r[3 + i];
+            t.sid[i] = v;
+            t.smc[i] = r[3 + ns + i];
+            isv = side_of(t.g, v) != 0;
+        }
+        nv += __popc(__ballot_sync(kFull, isv));
+    }
+    t.ns = ns; t.nss[1] = nv; t.nss[0] = ns - nv;
+    const uint32_t* fr = r + 3 + 2 * ns;
+    Hdr h = read_hdr(fr);
+    h.off[0] = F_WORDS;
+    h.off[1] = F_WORDS + 2 * c0;
+    h.top = F_WORDS + 2 * (c0 + c1);
+    h.parent = kNoPos;
+    const uint32_t* lr = fr + F_WORDS;
+    for (uint32_t i = t.lane; i < 2 * (c0 + c1); i += 32) t.arena[F_WORDS + i] = lr[i];
+    if (t.lane == 0) write_hdr(t.arena, h);
+    __syncwarp();
+    run_dfs(t, o, 0, sb, lim);
+}
+
+}  // namespace warp
+}  // namespace gmk

@@ -1,13 +1,17 @@
-// libgmk.so: the C ABI of include/gmk.h over the sm_100a enumeration kernel.
+// libgmk.so: the C ABI of include/gmk.h over the sm_100a enumeration kernels.
 //
 // Host side: .graph.bin reading and CSR validation, device residency of the
-// graph, a cached per-graph workspace (search arenas, member buffers,
-// counters, record buffer), the persistent-kernel launch, and delivery of
-// result records to the caller's sink.  Device side: enumerate_kernel, one
-// search task per thread at a time, tasks taken from a device work queue.
+// graph and of its edge hash table, a cached per-device workspace (search
+// arenas, member buffers, split buffers, record buffer), the round loop of
+// persistent-kernel launches, and delivery of result records to the caller's
+// sink.  Device side: enumerate_warp_kernel (one search task per warp at a
+// time, tasks from a device work queue, unfinished search trees split into
+// the next round's tasks) and enumerate_kernel (one task per thread; kept as
+// a second, independent implementation for differential tests).
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -18,6 +22,7 @@
 
 #include "../../include/gmk.h"
 #include "enum_core.cuh"
+#include "enum_warp.cuh"
 
 namespace {
 
@@ -39,6 +44,12 @@ int cuda_fail(cudaError_t e, const char* what) {
 struct Counters {
     unsigned long long count, hash_sum, hash_xor, nodes, work, next_task, out_pos, tasks_done;
     int stop, error;
+    unsigned long long t0_ns;   // device clock at the first task (watchdog origin)
+};
+
+// Per-round queue and split-buffer counters of the warp engine.
+struct RoundCounters {
+    unsigned long long next_task, tasks_done, next_used, next_count;
 };
 
 constexpr int kBlock = 128;
@@ -84,6 +95,102 @@ enumerate_kernel(gmk::GraphView g, uint32_t k, Counters* ctr, uint32_t* arenas,
     gmk::flush(t, o);
 }
 
+constexpr int kWBlock = 128;                 // 4 warps per block
+constexpr int kWarpsPerBlock = kWBlock / 32;
+constexpr uint32_t kDefaultWarpArena = 1u << 18;
+
+struct WarpArgs {
+    gmk::GraphView g;
+    gmk::warp::EdgeHash eh;
+    uint32_t k;
+    Counters* ctr;
+    RoundCounters* rc;
+    uint32_t* arenas;
+    uint32_t arena_words;
+    uint32_t* sbuf;
+    uint32_t smax;
+    uint32_t pair_limit;
+    int round;                         // 0: root tasks; > 0: split records
+    unsigned long long n_tasks;        // root tasks (round 0)
+    unsigned long long queue_len;      // queue entries this launch hands out
+    uint32_t chunk, chunks_per_root;
+    const uint32_t* root_order;
+    const uint32_t* cur_words;         // round > 0: records
+    const unsigned long long* cur_idx;
+    gmk::warp::SplitBuf next;
+    uint32_t split_min_nodes;          // 0: never split
+    unsigned long long limit;
+    uint32_t* out_buf;
+    unsigned long long out_cap;
+    unsigned long long watchdog_ns;
+    uint32_t shard, nshards;
+};
+
+__global__ void __launch_bounds__(kWBlock) enumerate_warp_kernel(const WarpArgs a) {
+    __shared__ uint32_t s_sat[kWarpsPerBlock][gmk::kSatCap];
+    __shared__ uint32_t s_src[kWarpsPerBlock][gmk::warp::kSrcCap];
+    using namespace gmk::warp;
+    const uint32_t wib = threadIdx.x >> 5;
+    const uint32_t lane = lane_id();
+    const unsigned long long wid = (unsigned long long)blockIdx.x * kWarpsPerBlock + wib;
+    Counters* ctr = a.ctr;
+    gmk::Outputs o;
+    o.count = &ctr->count; o.hash_sum = &ctr->hash_sum; o.hash_xor = &ctr->hash_xor;
+    o.nodes = &ctr->nodes; o.work = &ctr->work; o.stop = &ctr->stop; o.error = &ctr->error;
+    o.limit = a.limit; o.out_buf = a.out_buf; o.out_pos = &ctr->out_pos; o.out_cap = a.out_cap;
+    o.deadline_ns = 0;
+    if (a.watchdog_ns) {
+        // the first warp of the first round fixes the origin of the watchdog
+        unsigned long long t0 = 0;
+        if (lane == 0) {
+            const unsigned long long now = gmk::now_ns();
+            const unsigned long long old = atomicCAS(&ctr->t0_ns, 0ull, now);
+            t0 = old ? old : now;
+        }
+        o.deadline_ns = bcast(t0) + a.watchdog_ns;
+    }
+    Ctx t;
+    t.g = a.g; t.eh = a.eh; t.k = a.k;
+    t.arena = a.arenas + wid * a.arena_words; t.cap = a.arena_words;
+    t.sid = a.sbuf + wid * 2ull * a.smax; t.smc = t.sid + a.smax; t.smax = a.smax;
+    t.ns = 0; t.nss[0] = t.nss[1] = 0;
+    t.scan_limit = a.pair_limit; t.err = 0;
+    t.cnt = t.hsum = t.hxor = t.nodes = 0; t.work = 0;
+    t.sat = s_sat[wib]; t.src = s_src[wib]; t.lane = lane;
+    RunLimits lim;
+    lim.split_min_nodes = a.split_min_nodes;
+    lim.queue = &a.rc->next_task;
+    lim.queue_len = a.queue_len;
+    const SplitBuf* sb = a.split_min_nodes ? &a.next : nullptr;
+    for (;;) {
+        unsigned long long j = 0;
+        int stop = 0;
+        if (lane == 0) {
+            stop = gmk::load_flag(o.stop);
+            if (!stop) j = atomicAdd(&a.rc->next_task, 1ull);
+        }
+        stop = bcast(stop);
+        j = bcast(j);
+        if (stop || j >= a.queue_len) break;
+        if (lane == 0) atomicAdd(&a.rc->tasks_done, 1ull);
+        if (a.round == 0) {
+            const unsigned long long id = j * a.nshards + a.shard;
+            const uint32_t r = (uint32_t)(id / a.chunks_per_root);
+            const uint32_t c = (uint32_t)(id % a.chunks_per_root);
+            const uint32_t root = a.root_order ? a.root_order[r] : r;
+            const uint32_t first = a.g.nl + c * a.chunk;
+            const unsigned long long end = (unsigned long long)first + a.chunk;
+            const uint32_t last = end < a.g.n ? (uint32_t)end : a.g.n;
+            run_root(t, o, root, first, last, sb, lim);
+        } else {
+            run_record(t, o, a.cur_words + a.cur_idx[j], sb, lim);
+        }
+        flush(t, o);
+        if (t.err) break;
+    }
+    flush(t, o);
+}
+
 bool read_file(const char* path, std::vector<uint32_t>& words) {
     FILE* fp = std::fopen(path, "rb");
     if (!fp) return false;
@@ -123,6 +230,9 @@ struct gmk_graph {
     Counters* d_ctr = nullptr;
     uint32_t* d_order = nullptr;
     size_t order_bytes = 0;
+    unsigned long long* d_eh = nullptr;   // edge hash: buckets of 4 keys
+    unsigned long long eh_bmask = 0;
+    RoundCounters* d_rc = nullptr;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
@@ -140,6 +250,11 @@ struct Workspace {
     size_t sbuf_bytes = 0;
     uint32_t* d_out = nullptr;
     size_t out_bytes = 0;
+    // two split buffers (this round's records, the next round's)
+    uint32_t* d_split_words[2] = {nullptr, nullptr};
+    size_t split_words_bytes[2] = {0, 0};
+    unsigned long long* d_split_idx[2] = {nullptr, nullptr};
+    size_t split_idx_bytes[2] = {0, 0};
 };
 constexpr int kMaxDevices = 64;
 Workspace g_ws[kMaxDevices];
@@ -191,6 +306,27 @@ int upload(const uint32_t* off, const uint32_t* adj, uint32_t n, uint32_t nl, in
         return bail(cuda_fail(e, "H2D adj"));
     if ((e = cudaMalloc(&g->d_ctr, sizeof(Counters))) != cudaSuccess)
         return bail(cuda_fail(e, "cudaMalloc(counters)"));
+    if ((e = cudaMalloc(&g->d_rc, sizeof(RoundCounters))) != cudaSuccess)
+        return bail(cuda_fail(e, "cudaMalloc(round counters)"));
+    // edge hash: at most two keys per four slots
+    {
+        const unsigned long long edges = off[nl];
+        unsigned long long buckets = 1;
+        while (buckets * 2 < edges) buckets <<= 1;
+        g->eh_bmask = buckets - 1;
+        const size_t bytes = buckets * 4 * sizeof(unsigned long long);
+        if ((e = cudaMalloc(&g->d_eh, bytes)) != cudaSuccess)
+            return bail(cuda_fail(e, "cudaMalloc(edge hash)"));
+        if ((e = cudaMemsetAsync(g->d_eh, 0xFF, bytes, g->stream)) != cudaSuccess)
+            return bail(cuda_fail(e, "memset(edge hash)"));
+        if (edges) {
+            const unsigned grid = (unsigned)((edges + 255) / 256);
+            gmk::warp::build_edge_hash<<<grid, 256, 0, g->stream>>>(g->d_off, g->d_adj, nl, g->d_eh,
+                                                                     g->eh_bmask);
+            if ((e = cudaGetLastError()) != cudaSuccess)
+                return bail(cuda_fail(e, "build_edge_hash"));
+        }
+    }
     if ((e = cudaStreamSynchronize(g->stream)) != cudaSuccess) return bail(cuda_fail(e, "upload"));
     *out = g;
     return GMK_OK;
@@ -280,6 +416,7 @@ void gmk_graph_free(gmk_graph* g) {
     cudaSetDevice(g->device);
     if (g->stream) cudaStreamSynchronize(g->stream);
     cudaFree(g->d_off); cudaFree(g->d_adj); cudaFree(g->d_ctr); cudaFree(g->d_order);
+    cudaFree(g->d_eh); cudaFree(g->d_rc);
     if (g->ev0) cudaEventDestroy(g->ev0);
     if (g->ev1) cudaEventDestroy(g->ev1);
     if (g->stream) cudaStreamDestroy(g->stream);
@@ -297,30 +434,45 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
     if (!g || !opts || !out) return GMK_E_INVAL;
     if (opts->k < 1 || opts->k > 15) return GMK_E_INVAL;
     if (opts->emit && !sink) return GMK_E_INVAL;
+    if (opts->schedule < GMK_SCHEDULE_PLAIN || opts->schedule > GMK_SCHEDULE_ORDERED)
+        return GMK_E_INVAL;
     if (opts->schedule == GMK_SCHEDULE_ORDERED && !opts->task_cost) return GMK_E_INVAL;
     if (opts->nshards && opts->shard >= opts->nshards) return GMK_E_INVAL;
+    if (opts->engine != GMK_ENGINE_WARP && opts->engine != GMK_ENGINE_THREAD) return GMK_E_INVAL;
     std::memset(out, 0, sizeof(*out));
     CK(cudaSetDevice(g->device));
     if (g->nl == 0 || g->n == g->nl) return GMK_OK;   // a side is empty: no k-biplex
 
+    const bool warp = opts->engine == GMK_ENGINE_WARP;
     cudaDeviceProp prop;
     CK(cudaGetDeviceProperties(&prop, g->device));
     int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, enumerate_kernel, kBlock, 0));
+    if (warp)
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, enumerate_warp_kernel, kWBlock, 0));
+    else
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, enumerate_kernel, kBlock, 0));
     per_sm = std::max(per_sm, 1);
-    const uint32_t arena_words = opts->arena_words ? opts->arena_words : kDefaultArena;
+    const int block = warp ? kWBlock : kBlock;
+    const uint32_t lanes_per_worker = warp ? 32u : 1u;
+    const uint32_t arena_words =
+        opts->arena_words ? opts->arena_words : (warp ? kDefaultWarpArena : kDefaultArena);
     const uint32_t smax = opts->max_members ? opts->max_members : kDefaultSmax;
+    // workers: threads (thread engine) or warps (warp engine)
     uint64_t threads = opts->threads ? opts->threads
-                                     : (uint64_t)prop.multiProcessorCount * per_sm * kBlock;
+                                     : (uint64_t)prop.multiProcessorCount * per_sm * block;
+    threads = std::max<uint64_t>(threads, (uint64_t)block);
     // keep the search arenas within 40% of free device memory
     size_t free_b = 0, total_b = 0;
     CK(cudaMemGetInfo(&free_b, &total_b));
-    const uint64_t per_thread = 4ull * arena_words + 8ull * smax;
+    const uint64_t per_worker = 4ull * arena_words + 8ull * smax;
     Workspace& ws = g_ws[g->device];
     std::lock_guard<std::mutex> lock(ws.mu);
     const uint64_t budget = (uint64_t)((double)(free_b + ws.arena_bytes + ws.sbuf_bytes) * 0.4);
-    if (threads * per_thread > budget) threads = std::max<uint64_t>(kBlock, budget / per_thread);
-    threads = (threads + kBlock - 1) / kBlock * kBlock;
+    uint64_t workers = threads / lanes_per_worker;
+    if (workers * per_worker > budget)
+        workers = std::max<uint64_t>(block / lanes_per_worker, budget / per_worker);
+    threads = (workers * lanes_per_worker + block - 1) / block * block;
+    workers = threads / lanes_per_worker;
 
     // tasks: root x, chunk of first-level children
     const uint32_t nv = g->n - g->nl;
@@ -329,8 +481,8 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
         if (opts->chunk) {
             chunk = std::min(opts->chunk, nv);
         } else {
-            // about 8 tasks per thread, but no chunk below 16 children
-            const uint64_t want = 8ull * threads;
+            // about 8 tasks per worker, but no chunk below 16 children
+            const uint64_t want = 8ull * workers;
             const uint64_t per_root = (want + g->nl - 1) / g->nl;
             chunk = (uint32_t)std::max<uint64_t>(16, (nv + per_root - 1) / std::max<uint64_t>(1, per_root));
             chunk = std::min(chunk, nv);
@@ -338,10 +490,12 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
     }
     const uint32_t chunks_per_root = (nv + chunk - 1) / chunk;
     const unsigned long long n_tasks = (unsigned long long)g->nl * chunks_per_root;
+    const uint32_t nsh = opts->nshards ? opts->nshards : 1u, sh = opts->nshards ? opts->shard : 0u;
+    const unsigned long long my_tasks = n_tasks > sh ? (n_tasks - sh + nsh - 1) / nsh : 0;
 
     int rc;
-    if ((rc = grow((void**)&ws.d_arena, &ws.arena_bytes, threads * 4ull * arena_words))) return rc;
-    if ((rc = grow((void**)&ws.d_sbuf, &ws.sbuf_bytes, threads * 8ull * smax))) return rc;
+    if ((rc = grow((void**)&ws.d_arena, &ws.arena_bytes, workers * 4ull * arena_words))) return rc;
+    if ((rc = grow((void**)&ws.d_sbuf, &ws.sbuf_bytes, workers * 8ull * smax))) return rc;
     const uint32_t* d_order = nullptr;
     if (opts->schedule == GMK_SCHEDULE_ORDERED) {
         std::vector<uint32_t> order(g->nl);
@@ -358,21 +512,102 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
         out_words = opts->out_words ? opts->out_words : (64ull << 20);
         if ((rc = grow((void**)&ws.d_out, &ws.out_bytes, out_words * 4ull))) return rc;
     }
+    // the warp engine splits unfinished trees (batched / ordered schedules)
+    const uint32_t split_min = (!warp || opts->schedule == GMK_SCHEDULE_PLAIN)
+                                   ? 0u
+                                   : (opts->split_min_nodes ? opts->split_min_nodes : 64u);
+    unsigned long long split_word_cap = 0, split_idx_cap = 0;
+    if (split_min) {
+        split_word_cap = std::max<unsigned long long>(1ull << 22, workers * 4096ull);
+        split_idx_cap = std::max<unsigned long long>(1ull << 16, workers * 64ull);
+        for (int b = 0; b < 2; ++b) {
+            if ((rc = grow((void**)&ws.d_split_words[b], &ws.split_words_bytes[b], split_word_cap * 4)))
+                return rc;
+            if ((rc = grow((void**)&ws.d_split_idx[b], &ws.split_idx_bytes[b], split_idx_cap * 8)))
+                return rc;
+        }
+    }
     CK(cudaMemsetAsync(g->d_ctr, 0, sizeof(Counters), g->stream));
     gmk::GraphView gv{g->d_off, g->d_adj, g->n, g->nl};
-    const unsigned grid = (unsigned)(threads / kBlock);
-    CK(cudaEventRecord(g->ev0, g->stream));
-    enumerate_kernel<<<grid, kBlock, 0, g->stream>>>(
-        gv, opts->k, g->d_ctr, ws.d_arena, arena_words, ws.d_sbuf, smax,
-        opts->pair_limit ? opts->pair_limit : kDefaultPairLimit, n_tasks, chunk, chunks_per_root,
-        d_order, opts->result_limit, opts->emit ? ws.d_out : nullptr, out_words,
-        (unsigned long long)opts->watchdog_ms * 1000000ull, opts->nshards ? opts->shard : 0u,
-        opts->nshards ? opts->nshards : 1u);
-    CK(cudaGetLastError());
-    CK(cudaEventRecord(g->ev1, g->stream));
+    const unsigned grid = (unsigned)(threads / block);
+    const unsigned long long watchdog_ns = (unsigned long long)opts->watchdog_ms * 1000000ull;
+    const uint32_t pair_limit = opts->pair_limit ? opts->pair_limit : kDefaultPairLimit;
     Counters h;
-    CK(cudaMemcpyAsync(&h, g->d_ctr, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
-    CK(cudaStreamSynchronize(g->stream));
+    unsigned long long tasks_total = 0, tasks_done = 0;
+    uint32_t rounds = 0;
+    CK(cudaEventRecord(g->ev0, g->stream));
+    if (!warp) {
+        enumerate_kernel<<<grid, kBlock, 0, g->stream>>>(
+            gv, opts->k, g->d_ctr, ws.d_arena, arena_words, ws.d_sbuf, smax, pair_limit, n_tasks,
+            chunk, chunks_per_root, d_order, opts->result_limit, opts->emit ? ws.d_out : nullptr,
+            out_words, watchdog_ns, sh, nsh);
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(g->ev1, g->stream));
+        CK(cudaMemcpyAsync(&h, g->d_ctr, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
+        CK(cudaStreamSynchronize(g->stream));
+        tasks_total = my_tasks;
+        tasks_done = std::min<unsigned long long>(h.tasks_done, my_tasks);
+        rounds = 1;
+    } else {
+        WarpArgs a;
+        a.g = gv;
+        a.eh.slots = g->d_eh;
+        a.eh.bmask = g->eh_bmask;
+        a.k = opts->k;
+        a.ctr = g->d_ctr;
+        a.rc = g->d_rc;
+        a.arenas = ws.d_arena;
+        a.arena_words = arena_words;
+        a.sbuf = ws.d_sbuf;
+        a.smax = smax;
+        a.pair_limit = pair_limit;
+        a.n_tasks = n_tasks;
+        a.chunk = chunk;
+        a.chunks_per_root = chunks_per_root;
+        a.root_order = d_order;
+        a.split_min_nodes = split_min;
+        a.limit = opts->result_limit;
+        a.out_buf = opts->emit ? ws.d_out : nullptr;
+        a.out_cap = out_words;
+        a.watchdog_ns = watchdog_ns;
+        a.shard = sh;
+        a.nshards = nsh;
+        unsigned long long queue_len = my_tasks;
+        int cur = 0;
+        const auto host_t0 = std::chrono::steady_clock::now();
+        for (int round = 0;; ++round) {
+            a.round = round;
+            a.queue_len = queue_len;
+            a.cur_words = round ? ws.d_split_words[cur] : nullptr;
+            a.cur_idx = round ? ws.d_split_idx[cur] : nullptr;
+            a.next.words = ws.d_split_words[cur ^ 1];
+            a.next.idx = ws.d_split_idx[cur ^ 1];
+            a.next.used = &g->d_rc->next_used;
+            a.next.count = &g->d_rc->next_count;
+            a.next.word_cap = split_word_cap;
+            a.next.idx_cap = split_idx_cap;
+            CK(cudaMemsetAsync(g->d_rc, 0, sizeof(RoundCounters), g->stream));
+            enumerate_warp_kernel<<<grid, kWBlock, 0, g->stream>>>(a);
+            CK(cudaGetLastError());
+            RoundCounters r;
+            CK(cudaMemcpyAsync(&r, g->d_rc, sizeof(r), cudaMemcpyDeviceToHost, g->stream));
+            CK(cudaMemcpyAsync(&h, g->d_ctr, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
+            CK(cudaStreamSynchronize(g->stream));
+            ++rounds;
+            tasks_total += queue_len;
+            tasks_done += std::min<unsigned long long>(r.tasks_done, queue_len);
+            if (h.error || h.stop || r.next_count == 0) break;
+            if (watchdog_ns) {
+                const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() -
+                                                                host_t0).count();
+                if (el * 1e9 > (double)watchdog_ns) { h.error = gmk::TASK_E_TIMEOUT; break; }
+            }
+            queue_len = r.next_count;
+            cur ^= 1;
+        }
+        CK(cudaEventRecord(g->ev1, g->stream));
+        CK(cudaStreamSynchronize(g->stream));
+    }
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
 
@@ -381,12 +616,12 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
     out->hash_xor = h.hash_xor;
     out->nodes = h.nodes;
     out->algo_bytes = 4ull * h.work;
-    const uint32_t nsh = opts->nshards ? opts->nshards : 1u, sh = opts->nshards ? opts->shard : 0u;
-    out->tasks = n_tasks > sh ? (n_tasks - sh + nsh - 1) / nsh : 0;
-    out->tasks_done = std::min<unsigned long long>(h.tasks_done, out->tasks);
+    out->tasks = tasks_total;
+    out->tasks_done = tasks_done;
     out->kernel_ms = ms;
     out->truncated = opts->result_limit && h.count >= opts->result_limit;
     out->threads = (uint32_t)threads;
+    out->rounds = rounds;
     switch (h.error) {
         case gmk::TASK_OK: break;
         case gmk::TASK_E_ARENA: return GMK_E_ARENA;

@@ -6,7 +6,9 @@
 //   -m / -g are accepted and ignored (verbose dump / unused group size).
 // Output: "Result N: X: x1 x2 | Y: y1 y2 " lines when -q 1 (format of
 // reference include/output.cuh:102-145), then "Running Time: <ms> ms".
-// Extra: --all (no result limit), --schedule plain|batched, --stats.
+// Extra: --all (no result limit), --schedule plain|batched, --stats,
+// --threads N / --arena WORDS (resident search threads, per-worker arena),
+// --engine warp|thread.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -33,7 +35,8 @@ int print_result(void* user, const uint32_t* x, uint32_t nx, const uint32_t* y, 
 void usage() {
     std::fprintf(stderr,
                  "usage: gmk -f <graph.bin> [-k K] [-r LIMIT] [-q 0|1] [-d DEV] [--all]\n"
-                 "           [--schedule plain|batched] [--stats]\n");
+                 "           [--schedule plain|batched] [--stats] [--threads N] [--arena WORDS]\n"
+                 "           [--engine warp|thread]\n");
 }
 
 }  // namespace
@@ -57,6 +60,12 @@ int main(int argc, char** argv) {
         else if (!std::strcmp(argv[i], "-m") || !std::strcmp(argv[i], "-g")) (void)val(argv[i]);
         else if (!std::strcmp(argv[i], "--all")) o.result_limit = 0;
         else if (!std::strcmp(argv[i], "--stats")) stats = 1;
+        else if (!std::strcmp(argv[i], "--threads"))
+            o.threads = (uint32_t)std::strtoul(val("--threads"), nullptr, 10);
+        else if (!std::strcmp(argv[i], "--engine"))
+            o.engine = !std::strcmp(val("--engine"), "thread") ? GMK_ENGINE_THREAD : GMK_ENGINE_WARP;
+        else if (!std::strcmp(argv[i], "--arena"))
+            o.arena_words = (uint32_t)std::strtoul(val("--arena"), nullptr, 10);
         else if (!std::strcmp(argv[i], "--schedule")) {
             const char* s = val("--schedule");
             o.schedule = !std::strcmp(s, "plain") ? GMK_SCHEDULE_PLAIN : GMK_SCHEDULE_BATCHED;
@@ -96,10 +105,11 @@ int main(int argc, char** argv) {
     }
     std::printf("Running Time: %.3f ms\n", st.kernel_ms);
     if (stats)
-        std::printf("results %llu hash_sum %016llx hash_xor %016llx nodes %llu tasks %llu threads %u\n",
+        std::printf("results %llu hash_sum %016llx hash_xor %016llx nodes %llu tasks %llu threads %u "
+                    "rounds %u\n",
                     (unsigned long long)st.count, (unsigned long long)st.hash_sum,
                     (unsigned long long)st.hash_xor, (unsigned long long)st.nodes,
-                    (unsigned long long)st.tasks, st.threads);
+                    (unsigned long long)st.tasks, st.threads, st.rounds);
     gmk_graph_free(g);
     return 0;
 }

@@ -19,7 +19,7 @@
 extern "C" {
 #endif
 
-#define GMK_ABI_VERSION 1
+#define GMK_ABI_VERSION 2
 
 enum {
     GMK_OK = 0,
@@ -58,9 +58,16 @@ void gmk_graph_free(gmk_graph* g);
 /* Schedules of the search tasks (one task = a root U vertex and a chunk of its
  * first-level children). */
 enum {
-    GMK_SCHEDULE_PLAIN = 0,    /* one task per root, roots in id order */
-    GMK_SCHEDULE_BATCHED = 1,  /* roots split into chunks, persistent work queue */
-    GMK_SCHEDULE_ORDERED = 2   /* batched, tasks ordered by a caller-given cost (longest first) */
+    GMK_SCHEDULE_PLAIN = 0,    /* one task per root, roots in id order, no splitting */
+    GMK_SCHEDULE_BATCHED = 1,  /* roots split into chunks, persistent work queue; unfinished
+                                  search trees are split into the next round's tasks */
+    GMK_SCHEDULE_ORDERED = 2   /* batched, roots ordered by a caller-given cost (largest first) */
+};
+
+/* Search engines (same rules, same result set). */
+enum {
+    GMK_ENGINE_WARP = 0,       /* one task per warp, lanes share each node's work (default) */
+    GMK_ENGINE_THREAD = 1      /* one task per thread, no splitting */
 };
 
 typedef struct {
@@ -79,6 +86,9 @@ typedef struct {
                                  (|S|+|C_U|)*(|S|+|C_V|) <= pair_limit; 0 = 4096 */
     uint32_t shard, nshards;  /* run only tasks t with t % nshards == shard (one GPU of
                                  several); nshards 0 or 1 = all tasks */
+    int32_t engine;           /* GMK_ENGINE_* */
+    uint32_t split_min_nodes; /* warp engine, batched/ordered: a task is split only after this
+                                 many nodes; 0 = 64 */
 } gmk_opts;
 
 typedef struct {
@@ -92,6 +102,7 @@ typedef struct {
     double kernel_ms;         /* device time of the enumeration kernel (CUDA events) */
     int32_t truncated;        /* 1 if result_limit stopped the search */
     uint32_t threads;         /* search threads used */
+    uint32_t rounds;          /* kernel launches (rounds of split tasks) */
 } gmk_stats;
 
 /* Called from the calling thread after the kernel finished, once per result;

@@ -50,6 +50,27 @@ def test_schedule_does_not_change_the_set(golden, graphs, schedule, chunk):
     assert st.summary() == _summary(case)
 
 
+@pytest.mark.parametrize("split_min_nodes", [1, 7])
+def test_tree_splitting_does_not_change_the_set(golden, graphs, split_min_nodes):
+    # a tiny split threshold splits almost every task into the next round
+    for name, k in [("southernwomen", 2), ("er60", 2), ("er200", 1)]:
+        case = next(c for c in golden["cases"] if c["graph"] == name and c["k"] == k)
+        st = graphs(name).enumerate(k=k, chunk=2, split_min_nodes=split_min_nodes)
+        assert st.summary() == _summary(case), (name, k, split_min_nodes)
+        assert st.rounds >= 1
+
+
+@pytest.mark.parametrize("k", [1, 2])
+def test_thread_engine_matches_warp_engine(golden, graphs, k):
+    for name in ("southernwomen", "er60", "crime"):
+        hit = [c for c in golden["cases"] if c["graph"] == name and c["k"] == k]
+        st_t = graphs(name).enumerate(k=k, engine="thread")
+        st_w = graphs(name).enumerate(k=k, engine="warp")
+        assert st_t.summary() == st_w.summary(), name
+        if hit:
+            assert st_w.summary() == _summary(hit[0]), name
+
+
 def test_ordered_schedule_same_set(golden, graphs):
     case = next(c for c in golden["cases"] if c["graph"] == "er60" and c["k"] == 2)
     g = graphs("er60")
@@ -77,9 +98,12 @@ def test_emitted_sets_equal_reference_sets(graphs):
 
 @pytest.mark.parametrize("k", [1, 2, 3])
 def test_random_graphs_against_oracle(k):
+    # the search tree grows steeply with k; sides are kept small enough that
+    # the oracle finishes each graph in well under a second
+    hi = {1: 25, 2: 20, 3: 12}[k]
     for seed in range(12):
         rng = np.random.default_rng(100 + seed)
-        nu, nv = int(rng.integers(3, 25)), int(rng.integers(3, 25))
+        nu, nv = int(rng.integers(3, hi)), int(rng.integers(3, hi))
         g = gg.erdos_renyi(nu, nv, float(rng.uniform(0.1, 0.5)), 100 + seed)
         if g.n_left in (0, g.n):
             continue

@@ -174,8 +174,7 @@ def run_gmk(args, world, rank, local):
     off_np = off.numpy().view(np.uint32)
     adj_np = adj.numpy().view(np.uint32)
     h2d = 4 * (off_np.size + adj_np.size)
-    d2h = 80   # the counters record read back by gmk_enumerate
-    kw = dict(k=args.k, result_limit=args.limit, schedule=args.schedule)
+    kw = dict(k=args.k, result_limit=args.limit, schedule=args.schedule, engine=args.engine)
     if world > 1:
         kw.update(shard=rank, nshards=world)
 
@@ -191,7 +190,7 @@ def run_gmk(args, world, rank, local):
     barrier()
     clocks = ClockSampler(local)
     clocks.start()
-    ms, count, algo = [], 0, 0
+    ms, count, algo, launches = [], 0, 0, 0
     for _ in range(args.steps):
         flush_buf.zero_()          # L2 flush, outside the timed kernel
         torch.cuda.synchronize()
@@ -199,10 +198,19 @@ def run_gmk(args, world, rank, local):
         ms.append(st.kernel_ms)
         count += st.count
         algo += st.algo_bytes
+        launches += st.rounds
     barrier()
     clk = clocks.stop()
+    # the plain static schedule on the same GPU (one task per root, no splitting)
+    plain = None
+    if args.schedule != "plain" and not args.no_plain:
+        flush_buf.zero_()
+        torch.cuda.synchronize()
+        sp = dg.enumerate(**dict(kw, schedule="plain"))
+        plain = {"value": sp.count / (sp.kernel_ms / 1e3), "ms": sp.kernel_ms,
+                 "results": sp.count}
     # end to end through the C ABI: host CSR -> device, enumerate, read back
-    e2e_s = 0.0
+    e2e_s, e2e_rounds = 0.0, 0
     for _ in range(args.steps):
         flush_buf.zero_()
         barrier()
@@ -211,17 +219,19 @@ def run_gmk(args, world, rank, local):
         st2 = g2.enumerate(**kw)
         g2.close()
         e2e_s += time.perf_counter() - t0
+        e2e_rounds += st2.rounds
     barrier()
     tot_ms = sum(ms)
-    t = torch.tensor([tot_ms, e2e_s, float(count)], dtype=torch.float64, device=f"cuda:{local}")
     if world > 1:
-        mx = t.clone()
-        torch.distributed.all_reduce(mx, op=torch.distributed.ReduceOp.MAX)
-        sm = t.clone()
-        torch.distributed.all_reduce(sm, op=torch.distributed.ReduceOp.SUM)
-        tot_ms_max, e2e_max, count_all = mx[0].item(), mx[1].item(), sm[2].item()
+        from gmkbe_b200.shard import combine_max, combine_summary
+        dev = f"cuda:{local}"
+        tot_ms_max = combine_max(tot_ms, device=dev)
+        e2e_max = combine_max(e2e_s, device=dev)
+        count_all = float(combine_summary(count, 0, 0, device=dev)[0])
     else:
         tot_ms_max, e2e_max, count_all = tot_ms, e2e_s, float(count)
+    # counters read back after every round: 32 B round counters + 88 B totals
+    d2h = 120 * e2e_rounds / max(1, args.steps)
     if rank == 0:
         peak, peak_kind = _peaks()
         achieved = (algo / args.steps) / (tot_ms / args.steps / 1e3) / 1e9
@@ -235,15 +245,18 @@ def run_gmk(args, world, rank, local):
                        "parallelism": f"task shards x{world}" if world > 1 else "1 GPU"},
             "e2e": {"value": count_all / e2e_max, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
-            "gpu_launches": args.steps,
+            "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": _traffic_per_launch(),
                          "peak_source": peak_kind,
-                         "kernel": "enumerate_kernel",
+                         "kernel": ("enumerate_warp_kernel" if args.engine == "warp"
+                                    else "enumerate_kernel"),
                          "algorithmic_bytes_per_launch": algo / args.steps},
             "clocks": clk,
             "stats": {"nodes_per_step": st.nodes, "tasks": st.tasks, "tasks_done": st.tasks_done,
-                      "threads": st.threads},
+                      "threads": st.threads, "rounds_per_step": launches / args.steps,
+                      "engine": args.engine},
+            "plain_schedule": plain,
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args.k)
@@ -262,7 +275,9 @@ def main():
     ap.add_argument("--k", type=int, default=1)
     ap.add_argument("--limit", type=int, default=1_000_000)
     ap.add_argument("--schedule", default="batched", choices=["plain", "batched"])
+    ap.add_argument("--engine", default="warp", choices=["warp", "thread"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-schedule comparison")
     args = ap.parse_args()
     world, rank, local = _dist()
     if args.impl == "reference":

@@ -22,14 +22,18 @@ LIB_PATH = os.path.join(_PKG, "libgmk.so")
 
 # entry points declared in include/gmk.h
 EXPORTS = ("gmk_graph_load", "gmk_graph_from_csr", "gmk_graph_info", "gmk_graph_free",
-           "gmk_opts_default", "gmk_enumerate", "gmk_result_hash", "gmk_strerror",
-           "gmk_last_cuda_error", "gmk_abi_version")
+           "gmk_opts_default", "gmk_enumerate", "gmk_enumerate_resumable",
+           "gmk_result_hash", "gmk_strerror", "gmk_last_cuda_error",
+           "gmk_abi_version", "gmk_root_features", "gmk_mlp_create", "gmk_mlp_free",
+           "gmk_mlp_params", "gmk_mlp_gradient", "gmk_mlp_train", "gmk_mlp_predict")
 
 SCHEDULES = {"plain": 0, "batched": 1, "ordered": 2}
 ENGINES = {"warp": 0, "thread": 1}
 
 E_OUTBUF = -9
 E_SINK = -10
+E_CHECKPOINT = -12
+PAUSED = 1
 
 
 class GmkError(RuntimeError):
@@ -46,7 +50,9 @@ class _Opts(ctypes.Structure):
                 ("watchdog_ms", ctypes.c_uint32), ("out_words", ctypes.c_uint64),
                 ("task_cost", ctypes.POINTER(ctypes.c_float)), ("pair_limit", ctypes.c_uint32),
                 ("shard", ctypes.c_uint32), ("nshards", ctypes.c_uint32),
-                ("engine", ctypes.c_int32), ("split_min_nodes", ctypes.c_uint32)]
+                ("engine", ctypes.c_int32), ("split_min_nodes", ctypes.c_uint32),
+                ("root_begin", ctypes.c_uint32), ("root_end", ctypes.c_uint32),
+                ("root_nodes", ctypes.POINTER(ctypes.c_uint64))]
 
 
 class _Stats(ctypes.Structure):
@@ -83,6 +89,19 @@ def load_library(path: str = LIB_PATH):
     lib.gmk_opts_default.restype = None
     lib.gmk_enumerate.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Opts), SINK, ctypes.c_void_p,
                                   ctypes.POINTER(_Stats)]
+    lib.gmk_enumerate_resumable.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Opts), ctypes.c_char_p,
+                                            ctypes.c_uint32, ctypes.c_uint32, SINK,
+                                            ctypes.c_void_p, ctypes.POINTER(_Stats)]
+    PF = ctypes.POINTER(ctypes.c_float)
+    lib.gmk_root_features.argtypes = [ctypes.c_void_p, ctypes.c_uint32, PF]
+    lib.gmk_mlp_create.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)]
+    lib.gmk_mlp_free.argtypes = [ctypes.c_void_p]
+    lib.gmk_mlp_free.restype = None
+    lib.gmk_mlp_params.argtypes = [ctypes.c_void_p, PF, PF]
+    lib.gmk_mlp_gradient.argtypes = [ctypes.c_void_p, PF, PF, ctypes.c_uint32, PF, PF]
+    lib.gmk_mlp_train.argtypes = [ctypes.c_void_p, PF, PF, ctypes.c_uint32, ctypes.c_uint32,
+                                  ctypes.c_float, PF]
+    lib.gmk_mlp_predict.argtypes = [ctypes.c_void_p, PF, ctypes.c_uint32, PF]
     lib.gmk_result_hash.argtypes = [P32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                                     ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
     lib.gmk_result_hash.restype = None
@@ -180,14 +199,9 @@ class Graph:
     def __exit__(self, *a):
         self.close()
 
-    def enumerate(self, k: int = 1, result_limit: int = 0, schedule: str = "batched",
-                  collect: bool = False, chunk: int = 0, threads: int = 0, arena_words: int = 0,
-                  max_members: int = 0, watchdog_ms: int = 0, pair_limit: int = 0,
-                  task_cost=None, sink=None, shard: int = 0, nshards: int = 1,
-                  engine: str = "warp", split_min_nodes: int = 0) -> Stats:
-        """Enumerate maximal k-biplexes.  collect=True returns the result list
-        (sorted X, Y tuples) in Stats.results; `sink(x, y)` is called per
-        result otherwise (return True to stop)."""
+    def _opts(self, k, result_limit, schedule, chunk, threads, arena_words, max_members,
+              watchdog_ms, pair_limit, task_cost, shard, nshards, engine, split_min_nodes,
+              root_begin, root_end):
         lib = load_library()
         o = _Opts()
         lib.gmk_opts_default(ctypes.byref(o))
@@ -196,25 +210,57 @@ class Graph:
         o.max_members, o.watchdog_ms, o.pair_limit = max_members, watchdog_ms, pair_limit
         o.shard, o.nshards = shard, nshards
         o.engine, o.split_min_nodes = ENGINES[engine], split_min_nodes
+        o.root_begin, o.root_end = root_begin, root_end
         cost = None
         if task_cost is not None:
             cost = np.ascontiguousarray(task_cost, dtype=np.float32)
             if cost.size != self.n_left:
                 raise ValueError("task_cost needs one value per U vertex")
             o.task_cost = cost.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
-        out: list = []
-        cb = SINK(0)
-        if collect or sink is not None:
-            o.emit = 1
+        return o, cost
 
-            def _sink(_u, xp, nx, yp, ny):
-                x = tuple(xp[i] for i in range(nx))
-                y = tuple(yp[i] for i in range(ny))
-                if collect:
-                    out.append((x, y))
-                    return 0
-                return 1 if sink(x, y) else 0
-            cb = SINK(_sink)
+    @staticmethod
+    def _sink(collect, sink, out):
+        if not (collect or sink is not None):
+            return SINK(0)
+
+        def _cb(_u, xp, nx, yp, ny):
+            x = tuple(xp[i] for i in range(nx))
+            y = tuple(yp[i] for i in range(ny))
+            if collect:
+                out.append((x, y))
+                return 0
+            return 1 if sink(x, y) else 0
+        return SINK(_cb)
+
+    @staticmethod
+    def _stats(st, results):
+        return Stats(st.count, st.hash_sum, st.hash_xor, st.nodes, st.algo_bytes, st.tasks,
+                     st.tasks_done, st.kernel_ms, bool(st.truncated), st.threads, st.rounds,
+                     results)
+
+    def enumerate(self, k: int = 1, result_limit: int = 0, schedule: str = "batched",
+                  collect: bool = False, chunk: int = 0, threads: int = 0, arena_words: int = 0,
+                  max_members: int = 0, watchdog_ms: int = 0, pair_limit: int = 0,
+                  task_cost=None, sink=None, shard: int = 0, nshards: int = 1,
+                  engine: str = "warp", split_min_nodes: int = 0, root_begin: int = 0,
+                  root_end: int = 0, root_nodes=None) -> Stats:
+        """Enumerate maximal k-biplexes.  collect=True returns the result list
+        (sorted X, Y tuples) in Stats.results; `sink(x, y)` is called per
+        result otherwise (return True to stop).  root_nodes: a uint64 numpy
+        array of n_left entries to which each root's search nodes are added."""
+        lib = load_library()
+        o, _cost = self._opts(k, result_limit, schedule, chunk, threads, arena_words, max_members,
+                              watchdog_ms, pair_limit, task_cost, shard, nshards, engine,
+                              split_min_nodes, root_begin, root_end)
+        if root_nodes is not None:
+            if root_nodes.dtype != np.uint64 or root_nodes.size != self.n_left or \
+                    not root_nodes.flags.c_contiguous:
+                raise ValueError("root_nodes must be a contiguous uint64 array of n_left entries")
+            o.root_nodes = root_nodes.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+        out: list = []
+        cb = self._sink(collect, sink, out)
+        o.emit = 1 if (collect or sink is not None) else 0
         st = _Stats()
         while True:
             out.clear()
@@ -224,6 +270,30 @@ class Graph:
             o.out_words = (o.out_words or (64 << 20)) * 4
         if rc != E_SINK:
             _check(rc)
-        return Stats(st.count, st.hash_sum, st.hash_xor, st.nodes, st.algo_bytes, st.tasks,
-                     st.tasks_done, st.kernel_ms, bool(st.truncated), st.threads, st.rounds,
-                     out if collect else None)
+        return self._stats(st, out if collect else None)
+
+    def enumerate_resumable(self, checkpoint: str, batch_roots: int = 0, max_batches: int = 0,
+                            k: int = 1, result_limit: int = 0, schedule: str = "batched",
+                            collect: bool = False, sink=None, task_cost=None,
+                            engine: str = "warp", **tuning) -> tuple[Stats, bool]:
+        """gmk_enumerate_resumable: batches of roots with a checkpoint file after
+        each.  Returns (totals of the whole run, paused); paused is True when
+        max_batches stopped the call with work left (call again to resume)."""
+        lib = load_library()
+        o, _cost = self._opts(k, result_limit, schedule, tuning.get("chunk", 0),
+                              tuning.get("threads", 0), tuning.get("arena_words", 0),
+                              tuning.get("max_members", 0), tuning.get("watchdog_ms", 0),
+                              tuning.get("pair_limit", 0), task_cost, tuning.get("shard", 0),
+                              tuning.get("nshards", 1), engine, tuning.get("split_min_nodes", 0),
+                              0, 0)
+        out: list = []
+        cb = self._sink(collect, sink, out)
+        o.emit = 1 if (collect or sink is not None) else 0
+        if o.emit:
+            o.out_words = tuning.get("out_words", 0)
+        st = _Stats()
+        rc = lib.gmk_enumerate_resumable(self._h, ctypes.byref(o), os.fsencode(checkpoint),
+                                         batch_roots, max_batches, cb, None, ctypes.byref(st))
+        if rc not in (0, PAUSED, E_SINK):
+            _check(rc)
+        return self._stats(st, out if collect else None), rc == PAUSED

@@ -940,9 +940,10 @@ struct RunLimits {
     unsigned long long queue_len;       // entries this warp's round hands out
 };
 
-// Depth-first search from the frame at arena offset 0.
-__device__ void run_dfs(Ctx& t, const Outputs& o, uint32_t first, const SplitBuf* sb,
-                        const RunLimits& lim) {
+// Depth-first search from the frame at arena offset 0; returns the nodes it
+// entered.
+__device__ unsigned long long run_dfs(Ctx& t, const Outputs& o, uint32_t first,
+                                      const SplitBuf* sb, const RunLimits& lim) {
     uint32_t cur = 0;
     uint32_t polls = 0;
     unsigned long long task_nodes = 0;
@@ -986,11 +987,12 @@ __device__ void run_dfs(Ctx& t, const Outputs& o, uint32_t first, const SplitBuf
         cur = ch;
     }
     pop_to(t, 0);
+    return task_nodes;
 }
 
 // Root task: x in U with its first-level children y in [first, last).
-__device__ void run_root(Ctx& t, const Outputs& o, uint32_t root, uint32_t first, uint32_t last,
-                         const SplitBuf* sb, const RunLimits& lim) {
+__device__ unsigned long long run_root(Ctx& t, const Outputs& o, uint32_t root, uint32_t first,
+                                       uint32_t last, const SplitBuf* sb, const RunLimits& lim) {
     t.ns = 0; t.nss[0] = t.nss[1] = 0;
     push_member(t, root, nullptr);
     Hdr h;
@@ -1007,15 +1009,15 @@ __device__ void run_root(Ctx& t, const Outputs& o, uint32_t root, uint32_t first
         }
     if (t.lane == 0) write_hdr(t.arena, h);
     __syncwarp();
-    run_dfs(t, o, first, sb, lim);
+    return run_dfs(t, o, first, sb, lim);
 }
 
-// Resumed task: a frame written by split_path.
-__device__ void run_record(Ctx& t, const Outputs& o, const uint32_t* r, const SplitBuf* sb,
-                           const RunLimits& lim) {
+// Resumed task: a frame written by split_path (its S starts with the root).
+__device__ unsigned long long run_record(Ctx& t, const Outputs& o, const uint32_t* r,
+                                         const SplitBuf* sb, const RunLimits& lim) {
     const uint32_t ns = r[0], c0 = r[1], c1 = r[2];
-    if (ns > t.smax) { fail(t, o, TASK_E_SMAX); return; }
-    if (F_WORDS + 2ull * (c0 + c1) > t.cap) { fail(t, o, TASK_E_ARENA); return; }
+    if (ns > t.smax) { fail(t, o, TASK_E_SMAX); return 0; }
+    if (F_WORDS + 2ull * (c0 + c1) > t.cap) { fail(t, o, TASK_E_ARENA); return 0; }
     uint32_t nv = 0;
     for (uint32_t base = 0; base < ns; base += 32) {
         const uint32_t i = base + t.lane;
@@ -1039,7 +1041,7 @@ __device__ void run_record(Ctx& t, const Outputs& o, const uint32_t* r, const Sp
     for (uint32_t i = t.lane; i < 2 * (c0 + c1); i += 32) t.arena[F_WORDS + i] = lr[i];
     if (t.lane == 0) write_hdr(t.arena, h);
     __syncwarp();
-    run_dfs(t, o, 0, sb, lim);
+    return run_dfs(t, o, 0, sb, lim);
 }
 
 }  // namespace warp

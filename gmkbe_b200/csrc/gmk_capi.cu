@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -23,6 +24,7 @@
 #include "../../include/gmk.h"
 #include "enum_core.cuh"
 #include "enum_warp.cuh"
+#include "mlp.cuh"
 
 namespace {
 
@@ -61,9 +63,9 @@ __global__ void __launch_bounds__(kBlock)
 enumerate_kernel(gmk::GraphView g, uint32_t k, Counters* ctr, uint32_t* arenas,
                  uint32_t arena_words, uint32_t* sbuf, uint32_t smax, uint32_t pair_limit,
                  unsigned long long n_tasks, uint32_t chunk, uint32_t chunks_per_root,
-                 const uint32_t* root_order, unsigned long long limit, uint32_t* out_buf,
-                 unsigned long long out_cap, unsigned long long watchdog_ns, uint32_t shard,
-                 uint32_t nshards) {
+                 const uint32_t* root_order, uint32_t root_base, unsigned long long limit,
+                 uint32_t* out_buf, unsigned long long out_cap, unsigned long long watchdog_ns,
+                 uint32_t shard, uint32_t nshards) {
     const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     gmk::Outputs o;
     o.count = &ctr->count; o.hash_sum = &ctr->hash_sum; o.hash_xor = &ctr->hash_xor;
@@ -82,7 +84,7 @@ enumerate_kernel(gmk::GraphView g, uint32_t k, Counters* ctr, uint32_t* arenas,
         const unsigned long long id = j * nshards + shard;
         if (id >= n_tasks) break;
         atomicAdd(&ctr->tasks_done, 1ull);
-        const uint32_t r = (uint32_t)(id / chunks_per_root);
+        const uint32_t r = root_base + (uint32_t)(id / chunks_per_root);
         const uint32_t c = (uint32_t)(id % chunks_per_root);
         const uint32_t root = root_order ? root_order[r] : r;
         const uint32_t first = g.nl + c * chunk;
@@ -115,6 +117,7 @@ struct WarpArgs {
     unsigned long long queue_len;      // queue entries this launch hands out
     uint32_t chunk, chunks_per_root;
     const uint32_t* root_order;
+    uint32_t root_base;                // first root position of this call
     const uint32_t* cur_words;         // round > 0: records
     const unsigned long long* cur_idx;
     gmk::warp::SplitBuf next;
@@ -124,6 +127,7 @@ struct WarpArgs {
     unsigned long long out_cap;
     unsigned long long watchdog_ns;
     uint32_t shard, nshards;
+    unsigned long long* root_nodes;    // optional per-root node log
 };
 
 __global__ void __launch_bounds__(kWBlock) enumerate_warp_kernel(const WarpArgs a) {
@@ -175,15 +179,18 @@ __global__ void __launch_bounds__(kWBlock) enumerate_warp_kernel(const WarpArgs 
         if (lane == 0) atomicAdd(&a.rc->tasks_done, 1ull);
         if (a.round == 0) {
             const unsigned long long id = j * a.nshards + a.shard;
-            const uint32_t r = (uint32_t)(id / a.chunks_per_root);
+            const uint32_t r = a.root_base + (uint32_t)(id / a.chunks_per_root);
             const uint32_t c = (uint32_t)(id % a.chunks_per_root);
             const uint32_t root = a.root_order ? a.root_order[r] : r;
             const uint32_t first = a.g.nl + c * a.chunk;
             const unsigned long long end = (unsigned long long)first + a.chunk;
             const uint32_t last = end < a.g.n ? (uint32_t)end : a.g.n;
-            run_root(t, o, root, first, last, sb, lim);
+            const unsigned long long nodes = run_root(t, o, root, first, last, sb, lim);
+            if (a.root_nodes && lane == 0) atomicAdd(a.root_nodes + root, nodes);
         } else {
-            run_record(t, o, a.cur_words + a.cur_idx[j], sb, lim);
+            const uint32_t* rec = a.cur_words + a.cur_idx[j];
+            const unsigned long long nodes = run_record(t, o, rec, sb, lim);
+            if (a.root_nodes && lane == 0) atomicAdd(a.root_nodes + rec[3], nodes);
         }
         flush(t, o);
         if (t.err) break;
@@ -225,6 +232,7 @@ struct gmk_graph {
     int device = 0;
     uint32_t n = 0, nl = 0;
     uint64_t adj_len = 0;
+    uint64_t fingerprint = 0;   // hash of the CSR (checkpoint identity)
     uint32_t* d_off = nullptr;
     uint32_t* d_adj = nullptr;
     Counters* d_ctr = nullptr;
@@ -232,6 +240,8 @@ struct gmk_graph {
     size_t order_bytes = 0;
     unsigned long long* d_eh = nullptr;   // edge hash: buckets of 4 keys
     unsigned long long eh_bmask = 0;
+    unsigned long long* d_root_nodes = nullptr;   // per-root node log (on demand)
+    __half* d_feat = nullptr;                     // root features (on demand)
     RoundCounters* d_rc = nullptr;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -288,6 +298,12 @@ int upload(const uint32_t* off, const uint32_t* adj, uint32_t n, uint32_t nl, in
     gmk_graph* g = new (std::nothrow) gmk_graph();
     if (!g) return GMK_E_NOMEM;
     g->device = device; g->n = n; g->nl = nl; g->adj_len = off[n];
+    {
+        uint64_t h = gmk::mix64(((uint64_t)n << 32) | nl);
+        for (uint32_t v = 0; v <= n; ++v) h = gmk::mix64(h ^ off[v]);
+        for (uint64_t p = 0; p < g->adj_len; ++p) h = gmk::mix64(h ^ adj[p]);
+        g->fingerprint = h;
+    }
     auto bail = [&](int code) { gmk_graph_free(g); return code; };
     cudaError_t e;
     if ((e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking)) != cudaSuccess)
@@ -354,6 +370,8 @@ const char* gmk_strerror(int code) {
         case GMK_E_OUTBUF: return "record buffer too small (raise out_words)";
         case GMK_E_SINK: return "stopped by the sink";
         case GMK_E_NODEV: return "no usable CUDA device";
+        case GMK_E_CHECKPOINT: return "checkpoint unreadable or written for another graph / k";
+        case GMK_PAUSED: return "paused (checkpoint written, work remains)";
         default: return "unknown error";
     }
 }
@@ -416,7 +434,7 @@ void gmk_graph_free(gmk_graph* g) {
     cudaSetDevice(g->device);
     if (g->stream) cudaStreamSynchronize(g->stream);
     cudaFree(g->d_off); cudaFree(g->d_adj); cudaFree(g->d_ctr); cudaFree(g->d_order);
-    cudaFree(g->d_eh); cudaFree(g->d_rc);
+    cudaFree(g->d_eh); cudaFree(g->d_rc); cudaFree(g->d_root_nodes); cudaFree(g->d_feat);
     if (g->ev0) cudaEventDestroy(g->ev0);
     if (g->ev1) cudaEventDestroy(g->ev1);
     if (g->stream) cudaStreamDestroy(g->stream);
@@ -439,9 +457,13 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
     if (opts->schedule == GMK_SCHEDULE_ORDERED && !opts->task_cost) return GMK_E_INVAL;
     if (opts->nshards && opts->shard >= opts->nshards) return GMK_E_INVAL;
     if (opts->engine != GMK_ENGINE_WARP && opts->engine != GMK_ENGINE_THREAD) return GMK_E_INVAL;
+    if (opts->root_nodes && opts->engine != GMK_ENGINE_WARP) return GMK_E_INVAL;
+    const uint32_t root_end = opts->root_end ? opts->root_end : g->nl;
+    if (root_end > g->nl || opts->root_begin > root_end) return GMK_E_INVAL;
+    const uint32_t root_begin = opts->root_begin;
     std::memset(out, 0, sizeof(*out));
     CK(cudaSetDevice(g->device));
-    if (g->nl == 0 || g->n == g->nl) return GMK_OK;   // a side is empty: no k-biplex
+    if (g->nl == 0 || g->n == g->nl || root_begin == root_end) return GMK_OK;   // nothing to do
 
     const bool warp = opts->engine == GMK_ENGINE_WARP;
     cudaDeviceProp prop;
@@ -489,7 +511,7 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
         }
     }
     const uint32_t chunks_per_root = (nv + chunk - 1) / chunk;
-    const unsigned long long n_tasks = (unsigned long long)g->nl * chunks_per_root;
+    const unsigned long long n_tasks = (unsigned long long)(root_end - root_begin) * chunks_per_root;
     const uint32_t nsh = opts->nshards ? opts->nshards : 1u, sh = opts->nshards ? opts->shard : 0u;
     const unsigned long long my_tasks = n_tasks > sh ? (n_tasks - sh + nsh - 1) / nsh : 0;
 
@@ -539,8 +561,8 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
     if (!warp) {
         enumerate_kernel<<<grid, kBlock, 0, g->stream>>>(
             gv, opts->k, g->d_ctr, ws.d_arena, arena_words, ws.d_sbuf, smax, pair_limit, n_tasks,
-            chunk, chunks_per_root, d_order, opts->result_limit, opts->emit ? ws.d_out : nullptr,
-            out_words, watchdog_ns, sh, nsh);
+            chunk, chunks_per_root, d_order, root_begin, opts->result_limit,
+            opts->emit ? ws.d_out : nullptr, out_words, watchdog_ns, sh, nsh);
         CK(cudaGetLastError());
         CK(cudaEventRecord(g->ev1, g->stream));
         CK(cudaMemcpyAsync(&h, g->d_ctr, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
@@ -565,6 +587,7 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
         a.chunk = chunk;
         a.chunks_per_root = chunks_per_root;
         a.root_order = d_order;
+        a.root_base = root_begin;
         a.split_min_nodes = split_min;
         a.limit = opts->result_limit;
         a.out_buf = opts->emit ? ws.d_out : nullptr;
@@ -572,6 +595,12 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
         a.watchdog_ns = watchdog_ns;
         a.shard = sh;
         a.nshards = nsh;
+        a.root_nodes = nullptr;
+        if (opts->root_nodes) {
+            if (!g->d_root_nodes) CK(cudaMalloc(&g->d_root_nodes, 8ull * g->nl));
+            CK(cudaMemsetAsync(g->d_root_nodes, 0, 8ull * g->nl, g->stream));
+            a.root_nodes = g->d_root_nodes;
+        }
         unsigned long long queue_len = my_tasks;
         int cur = 0;
         const auto host_t0 = std::chrono::steady_clock::now();
@@ -607,6 +636,11 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
         }
         CK(cudaEventRecord(g->ev1, g->stream));
         CK(cudaStreamSynchronize(g->stream));
+        if (opts->root_nodes) {
+            std::vector<unsigned long long> rn(g->nl);
+            CK(cudaMemcpy(rn.data(), g->d_root_nodes, 8ull * g->nl, cudaMemcpyDeviceToHost));
+            for (uint32_t i = 0; i < g->nl; ++i) opts->root_nodes[i] += rn[i];
+        }
     }
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
@@ -646,6 +680,320 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
         }
     }
     return GMK_OK;
+}
+
+// ---------------------------------------------------------------- learned schedule
+
+struct gmk_mlp {
+    int device = 0;
+    float* d_master = nullptr;   // FP32 master weights
+    __half* d_w = nullptr;       // FP16 working copy
+    float* d_m = nullptr;        // Adam moments
+    float* d_v = nullptr;
+    float* d_grad = nullptr;
+    float* d_loss = nullptr;
+    uint64_t steps = 0;
+    // per-call sample buffers, grown on demand
+    __half* d_x = nullptr;
+    float* d_xf = nullptr;
+    float* d_y = nullptr;
+    float* d_act = nullptr;
+    float* d_out = nullptr;
+    uint32_t cap = 0;
+};
+
+namespace {
+
+using gmk::mlp::NP;
+
+int mlp_reserve(gmk_mlp* m, uint32_t n) {
+    if (n <= m->cap) return GMK_OK;
+    cudaFree(m->d_x); cudaFree(m->d_xf); cudaFree(m->d_y); cudaFree(m->d_act); cudaFree(m->d_out);
+    m->d_x = nullptr; m->d_xf = nullptr; m->d_y = nullptr; m->d_act = nullptr; m->d_out = nullptr;
+    m->cap = 0;
+    const uint64_t nn = n;
+    CK(cudaMalloc(&m->d_x, nn * gmk::mlp::F * sizeof(__half)));
+    CK(cudaMalloc(&m->d_xf, nn * gmk::mlp::F * sizeof(float)));
+    CK(cudaMalloc(&m->d_y, nn * sizeof(float)));
+    CK(cudaMalloc(&m->d_act, nn * 2 * gmk::mlp::H * sizeof(float)));
+    CK(cudaMalloc(&m->d_out, nn * sizeof(float)));
+    m->cap = n;
+    return GMK_OK;
+}
+
+// Uploads n samples (features rounded to FP16 on the device) and, if y, targets.
+int mlp_upload(gmk_mlp* m, const float* x, const float* y, uint32_t n) {
+    if (int rc = mlp_reserve(m, n)) return rc;
+    const uint64_t nf = (uint64_t)n * gmk::mlp::F;
+    CK(cudaMemcpy(m->d_xf, x, nf * sizeof(float), cudaMemcpyHostToDevice));
+    gmk::mlp::float_to_half_kernel<<<(unsigned)((nf + 255) / 256), 256>>>(m->d_xf, m->d_x, nf);
+    CK(cudaGetLastError());
+    if (y) CK(cudaMemcpy(m->d_y, y, (uint64_t)n * sizeof(float), cudaMemcpyHostToDevice));
+    return GMK_OK;
+}
+
+// Forward + backward of the MSE over n uploaded samples into d_grad / d_loss.
+int mlp_grad(gmk_mlp* m, uint32_t n) {
+    CK(cudaMemset(m->d_grad, 0, NP * sizeof(float)));
+    CK(cudaMemset(m->d_loss, 0, sizeof(float)));
+    const unsigned grid = (n + gmk::mlp::kBlock - 1) / gmk::mlp::kBlock;
+    gmk::mlp::forward_kernel<<<grid, gmk::mlp::kBlock>>>(m->d_w, m->d_x, n, m->d_act, m->d_out);
+    CK(cudaGetLastError());
+    gmk::mlp::backward_kernel<<<grid, gmk::mlp::kBlock>>>(m->d_w, m->d_x, m->d_y, m->d_act,
+                                                         m->d_out, n, m->d_grad, m->d_loss);
+    CK(cudaGetLastError());
+    return GMK_OK;
+}
+
+}  // namespace
+
+int gmk_root_features(const gmk_graph* g, uint32_t k, float* out) {
+    if (!g || !out || k < 1) return GMK_E_INVAL;
+    CK(cudaSetDevice(g->device));
+    if (g->nl == 0) return GMK_OK;
+    gmk_graph* gm = const_cast<gmk_graph*>(g);
+    if (!gm->d_feat) CK(cudaMalloc(&gm->d_feat, (uint64_t)g->nl * gmk::mlp::F * sizeof(__half)));
+    gmk::GraphView gv{g->d_off, g->d_adj, g->n, g->nl};
+    const uint64_t threads = (uint64_t)g->nl * 32;
+    gmk::mlp::root_features_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, g->stream>>>(
+        gv, k, gm->d_feat);
+    CK(cudaGetLastError());
+    std::vector<__half> h((uint64_t)g->nl * gmk::mlp::F);
+    CK(cudaMemcpyAsync(h.data(), gm->d_feat, h.size() * sizeof(__half), cudaMemcpyDeviceToHost,
+                       g->stream));
+    CK(cudaStreamSynchronize(g->stream));
+    for (size_t i = 0; i < h.size(); ++i) out[i] = __half2float(h[i]);
+    return GMK_OK;
+}
+
+int gmk_mlp_create(int device, uint64_t seed, gmk_mlp** out) {
+    if (!out) return GMK_E_INVAL;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        g_cuda_err = "no CUDA device";
+        return GMK_E_NODEV;
+    }
+    if (device < 0 || device >= ndev) return GMK_E_INVAL;
+    CK(cudaSetDevice(device));
+    gmk_mlp* m = new (std::nothrow) gmk_mlp();
+    if (!m) return GMK_E_NOMEM;
+    m->device = device;
+    auto bail = [&](int code) { gmk_mlp_free(m); return code; };
+    cudaError_t e;
+    if ((e = cudaMalloc(&m->d_master, NP * sizeof(float))) != cudaSuccess ||
+        (e = cudaMalloc(&m->d_w, NP * sizeof(__half))) != cudaSuccess ||
+        (e = cudaMalloc(&m->d_m, NP * sizeof(float))) != cudaSuccess ||
+        (e = cudaMalloc(&m->d_v, NP * sizeof(float))) != cudaSuccess ||
+        (e = cudaMalloc(&m->d_grad, NP * sizeof(float))) != cudaSuccess ||
+        (e = cudaMalloc(&m->d_loss, sizeof(float))) != cudaSuccess)
+        return bail(cuda_fail(e, "cudaMalloc(mlp)"));
+    // He-uniform initialisation from a splitmix64 stream; biases zero
+    std::vector<float> w(NP, 0.f);
+    uint64_t st = seed;
+    auto uni = [&st]() {
+        st += 0x9E3779B97F4A7C15ull;
+        return (double)(gmk::mix64(st) >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+    };
+    const int H = gmk::mlp::H, F = gmk::mlp::F;
+    for (int i = 0; i < H * F; ++i) w[gmk::mlp::OFF_W1 + i] = (float)(uni() * std::sqrt(6.0 / F));
+    for (int i = 0; i < H * H; ++i) w[gmk::mlp::OFF_W2 + i] = (float)(uni() * std::sqrt(6.0 / H));
+    for (int i = 0; i < H; ++i) w[gmk::mlp::OFF_W3 + i] = (float)(uni() * std::sqrt(6.0 / H));
+    const int rc = gmk_mlp_params(m, nullptr, w.data());
+    if (rc) return bail(rc);
+    *out = m;
+    return GMK_OK;
+}
+
+void gmk_mlp_free(gmk_mlp* m) {
+    if (!m) return;
+    cudaSetDevice(m->device);
+    cudaFree(m->d_master); cudaFree(m->d_w); cudaFree(m->d_m); cudaFree(m->d_v);
+    cudaFree(m->d_grad); cudaFree(m->d_loss);
+    cudaFree(m->d_x); cudaFree(m->d_xf); cudaFree(m->d_y); cudaFree(m->d_act); cudaFree(m->d_out);
+    delete m;
+}
+
+int gmk_mlp_params(gmk_mlp* m, float* get, const float* set) {
+    if (!m) return GMK_E_INVAL;
+    CK(cudaSetDevice(m->device));
+    if (set) {
+        CK(cudaMemcpy(m->d_master, set, NP * sizeof(float), cudaMemcpyHostToDevice));
+        gmk::mlp::to_half_kernel<<<(NP + 255) / 256, 256>>>(m->d_master, m->d_w);
+        CK(cudaGetLastError());
+        CK(cudaMemset(m->d_m, 0, NP * sizeof(float)));
+        CK(cudaMemset(m->d_v, 0, NP * sizeof(float)));
+        m->steps = 0;
+    }
+    if (get) CK(cudaMemcpy(get, m->d_master, NP * sizeof(float), cudaMemcpyDeviceToHost));
+    CK(cudaDeviceSynchronize());
+    return GMK_OK;
+}
+
+int gmk_mlp_gradient(gmk_mlp* m, const float* x, const float* y, uint32_t n, float* grad,
+                     float* loss) {
+    if (!m || !x || !y || n == 0) return GMK_E_INVAL;
+    CK(cudaSetDevice(m->device));
+    if (int rc = mlp_upload(m, x, y, n)) return rc;
+    if (int rc = mlp_grad(m, n)) return rc;
+    if (grad) CK(cudaMemcpy(grad, m->d_grad, NP * sizeof(float), cudaMemcpyDeviceToHost));
+    float l = 0.f;
+    CK(cudaMemcpy(&l, m->d_loss, sizeof(float), cudaMemcpyDeviceToHost));
+    if (loss) *loss = l;
+    return GMK_OK;
+}
+
+int gmk_mlp_train(gmk_mlp* m, const float* x, const float* y, uint32_t n, uint32_t epochs,
+                  float lr, float* loss) {
+    if (!m || !x || !y || n == 0) return GMK_E_INVAL;
+    CK(cudaSetDevice(m->device));
+    if (int rc = mlp_upload(m, x, y, n)) return rc;
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    for (uint32_t ep = 0; ep < epochs; ++ep) {
+        if (int rc = mlp_grad(m, n)) return rc;
+        ++m->steps;
+        const float c1 = 1.f - std::pow(b1, (float)m->steps);
+        const float c2 = 1.f - std::pow(b2, (float)m->steps);
+        gmk::mlp::adam_kernel<<<(NP + 255) / 256, 256>>>(m->d_master, m->d_w, m->d_grad, m->d_m,
+                                                         m->d_v, lr, b1, b2, eps, c1, c2);
+        CK(cudaGetLastError());
+    }
+    // loss of the final weights
+    if (int rc = mlp_grad(m, n)) return rc;
+    float l = 0.f;
+    CK(cudaMemcpy(&l, m->d_loss, sizeof(float), cudaMemcpyDeviceToHost));
+    if (loss) *loss = l;
+    return GMK_OK;
+}
+
+int gmk_mlp_predict(gmk_mlp* m, const float* x, uint32_t n, float* out) {
+    if (!m || !x || !out) return GMK_E_INVAL;
+    if (n == 0) return GMK_OK;
+    CK(cudaSetDevice(m->device));
+    if (int rc = mlp_upload(m, x, nullptr, n)) return rc;
+    const unsigned grid = (n + gmk::mlp::kBlock - 1) / gmk::mlp::kBlock;
+    gmk::mlp::forward_kernel<<<grid, gmk::mlp::kBlock>>>(m->d_w, m->d_x, n, nullptr, m->d_out);
+    CK(cudaGetLastError());
+    CK(cudaMemcpy(out, m->d_out, (uint64_t)n * sizeof(float), cudaMemcpyDeviceToHost));
+    return GMK_OK;
+}
+
+namespace {
+
+struct Checkpoint {
+    uint64_t fingerprint = 0;
+    uint32_t k = 0, schedule = 0, next_root = 0, done = 0;
+    uint64_t order_hash = 0, count = 0, hash_sum = 0, hash_xor = 0, nodes = 0;
+};
+
+bool read_checkpoint(const char* path, Checkpoint& c, bool& exists) {
+    FILE* fp = std::fopen(path, "r");
+    exists = fp != nullptr;
+    if (!fp) return false;
+    unsigned long long fpv = 0, oh = 0, cnt = 0, hs = 0, hx = 0, nd = 0;
+    unsigned k = 0, sch = 0, nr = 0, dn = 0;
+    const int got = std::fscanf(fp,
+                                "gmk-checkpoint 1\ngraph %llx\nk %u\nschedule %u\norder %llx\n"
+                                "next_root %u\ncount %llu\nhash_sum %llx\nhash_xor %llx\n"
+                                "nodes %llu\ndone %u\n",
+                                &fpv, &k, &sch, &oh, &nr, &cnt, &hs, &hx, &nd, &dn);
+    std::fclose(fp);
+    if (got != 10) return false;
+    c.fingerprint = fpv; c.k = k; c.schedule = sch; c.order_hash = oh; c.next_root = nr;
+    c.count = cnt; c.hash_sum = hs; c.hash_xor = hx; c.nodes = nd; c.done = dn;
+    return true;
+}
+
+bool write_checkpoint(const char* path, const Checkpoint& c) {
+    const std::string tmp = std::string(path) + ".tmp";
+    FILE* fp = std::fopen(tmp.c_str(), "w");
+    if (!fp) return false;
+    std::fprintf(fp,
+                 "gmk-checkpoint 1\ngraph %016llx\nk %u\nschedule %u\norder %016llx\n"
+                 "next_root %u\ncount %llu\nhash_sum %016llx\nhash_xor %016llx\nnodes %llu\n"
+                 "done %u\n",
+                 (unsigned long long)c.fingerprint, c.k, c.schedule,
+                 (unsigned long long)c.order_hash, c.next_root, (unsigned long long)c.count,
+                 (unsigned long long)c.hash_sum, (unsigned long long)c.hash_xor,
+                 (unsigned long long)c.nodes, c.done);
+    const bool ok = std::fflush(fp) == 0;
+    std::fclose(fp);
+    return ok && std::rename(tmp.c_str(), path) == 0;
+}
+
+uint64_t order_hash(const gmk_graph* g, const gmk_opts* o) {
+    if (o->schedule != GMK_SCHEDULE_ORDERED || !o->task_cost) return 0;
+    uint64_t h = 0x51ED270B7A3C2D1Full;
+    for (uint32_t i = 0; i < g->nl; ++i) {
+        uint32_t bits;
+        std::memcpy(&bits, o->task_cost + i, 4);
+        h = gmk::mix64(h ^ bits);
+    }
+    return h;
+}
+
+}  // namespace
+
+int gmk_enumerate_resumable(gmk_graph* g, const gmk_opts* opts, const char* checkpoint_path,
+                            uint32_t batch_roots, uint32_t max_batches, gmk_sink sink,
+                            void* user, gmk_stats* out) {
+    if (!g || !opts || !out || !checkpoint_path) return GMK_E_INVAL;
+    std::memset(out, 0, sizeof(*out));
+    Checkpoint c;
+    bool exists = false;
+    const uint64_t oh = order_hash(g, opts);
+    if (read_checkpoint(checkpoint_path, c, exists)) {
+        if (c.fingerprint != g->fingerprint || c.k != opts->k ||
+            c.schedule != (uint32_t)opts->schedule || c.order_hash != oh || c.next_root > g->nl)
+            return GMK_E_CHECKPOINT;
+    } else if (exists) {
+        return GMK_E_CHECKPOINT;
+    } else {
+        c.fingerprint = g->fingerprint;
+        c.k = opts->k;
+        c.schedule = (uint32_t)opts->schedule;
+        c.order_hash = oh;
+    }
+    const uint32_t batch = batch_roots ? batch_roots : std::max<uint32_t>(1, (g->nl + 63) / 64);
+    uint32_t batches = 0;
+    double ms = 0;
+    int rc = GMK_OK;
+    while (!c.done) {
+        const bool limit_hit = opts->result_limit && c.count >= opts->result_limit;
+        if (c.next_root >= g->nl || limit_hit) {
+            c.done = 1;
+            if (!write_checkpoint(checkpoint_path, c)) return GMK_E_IO;
+            break;
+        }
+        if (max_batches && batches >= max_batches) { rc = GMK_PAUSED; break; }
+        gmk_opts o = *opts;
+        o.root_begin = c.next_root;
+        o.root_end = (uint32_t)std::min<uint64_t>(g->nl, (uint64_t)c.next_root + batch);
+        o.result_limit = opts->result_limit ? opts->result_limit - c.count : 0;
+        gmk_stats st;
+        const int r = gmk_enumerate(g, &o, sink, user, &st);
+        if (r) return r;
+        c.count += st.count;
+        c.hash_sum += st.hash_sum;
+        c.hash_xor ^= st.hash_xor;
+        c.nodes += st.nodes;
+        c.next_root = o.root_end;
+        ms += st.kernel_ms;
+        out->algo_bytes += st.algo_bytes;
+        out->tasks += st.tasks;
+        out->tasks_done += st.tasks_done;
+        out->rounds += st.rounds;
+        out->threads = st.threads;
+        ++batches;
+        if (!write_checkpoint(checkpoint_path, c)) return GMK_E_IO;
+    }
+    out->count = c.count;
+    out->hash_sum = c.hash_sum;
+    out->hash_xor = c.hash_xor;
+    out->nodes = c.nodes;
+    out->kernel_ms = ms;
+    out->truncated = opts->result_limit && c.count >= opts->result_limit;
+    return rc;
 }
 
 }  // extern "C"

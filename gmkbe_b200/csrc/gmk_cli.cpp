@@ -8,7 +8,9 @@
 // reference include/output.cuh:102-145), then "Running Time: <ms> ms".
 // Extra: --all (no result limit), --schedule plain|batched, --stats,
 // --threads N / --arena WORDS (resident search threads, per-worker arena),
-// --engine warp|thread.
+// --engine warp|thread, --checkpoint FILE [--batch-roots N] (resumable run:
+// the file is rewritten after every batch of roots and a restarted command
+// continues from it).
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -36,7 +38,7 @@ void usage() {
     std::fprintf(stderr,
                  "usage: gmk -f <graph.bin> [-k K] [-r LIMIT] [-q 0|1] [-d DEV] [--all]\n"
                  "           [--schedule plain|batched] [--stats] [--threads N] [--arena WORDS]\n"
-                 "           [--engine warp|thread]\n");
+                 "           [--engine warp|thread] [--checkpoint FILE [--batch-roots N]]\n");
 }
 
 }  // namespace
@@ -47,6 +49,8 @@ int main(int argc, char** argv) {
     gmk_opts_default(&o);
     o.result_limit = 10000000ull;
     int quiet = 0, dev = 0, stats = 0;
+    std::string checkpoint;
+    uint32_t batch_roots = 0;
     for (int i = 1; i < argc; ++i) {
         auto val = [&](const char* name) -> const char* {
             if (i + 1 >= argc) { std::fprintf(stderr, "missing value for %s\n", name); std::exit(2); }
@@ -62,6 +66,9 @@ int main(int argc, char** argv) {
         else if (!std::strcmp(argv[i], "--stats")) stats = 1;
         else if (!std::strcmp(argv[i], "--threads"))
             o.threads = (uint32_t)std::strtoul(val("--threads"), nullptr, 10);
+        else if (!std::strcmp(argv[i], "--checkpoint")) checkpoint = val("--checkpoint");
+        else if (!std::strcmp(argv[i], "--batch-roots"))
+            batch_roots = (uint32_t)std::strtoul(val("--batch-roots"), nullptr, 10);
         else if (!std::strcmp(argv[i], "--engine"))
             o.engine = !std::strcmp(val("--engine"), "thread") ? GMK_ENGINE_THREAD : GMK_ENGINE_WARP;
         else if (!std::strcmp(argv[i], "--arena"))
@@ -93,7 +100,10 @@ int main(int argc, char** argv) {
     o.emit = quiet ? 1 : 0;
     gmk_stats st;
     for (;;) {
-        rc = gmk_enumerate(g, &o, quiet ? print_result : nullptr, &p, &st);
+        rc = checkpoint.empty()
+                 ? gmk_enumerate(g, &o, quiet ? print_result : nullptr, &p, &st)
+                 : gmk_enumerate_resumable(g, &o, checkpoint.c_str(), batch_roots, 0,
+                                           quiet ? print_result : nullptr, &p, &st);
         if (rc != GMK_E_OUTBUF) break;
         o.out_words = (o.out_words ? o.out_words : (64ull << 20)) * 4;   // retry, bigger buffer
         p.n = 0;

@@ -33,7 +33,9 @@ enum {
     GMK_E_TIMEOUT = -8,  /* watchdog_ms elapsed; counts cover the work done so far */
     GMK_E_OUTBUF = -9,   /* record buffer too small for emit mode; raise out_words */
     GMK_E_SINK = -10,    /* the sink asked to stop (not an error for the caller's data) */
-    GMK_E_NODEV = -11    /* no CUDA device / extension not usable */
+    GMK_E_NODEV = -11,   /* no CUDA device / extension not usable */
+    GMK_E_CHECKPOINT = -12, /* checkpoint file unreadable, or written for another graph / k */
+    GMK_PAUSED = 1       /* not an error: max_batches reached, the checkpoint holds the rest */
 };
 
 typedef struct gmk_graph gmk_graph;
@@ -89,6 +91,13 @@ typedef struct {
     int32_t engine;           /* GMK_ENGINE_* */
     uint32_t split_min_nodes; /* warp engine, batched/ordered: a task is split only after this
                                  many nodes; 0 = 64 */
+    uint32_t root_begin;      /* only roots at positions [root_begin, root_end) of the root
+                                 order (id order, or cost order for ORDERED); the ranges of */
+    uint32_t root_end;        /* consecutive calls partition the result set; root_end 0 = all.
+                                 Used for checkpoint / resume. */
+    uint64_t* root_nodes;     /* optional, warp engine: host array of n_left counters; the
+                                 search nodes of each root's tasks are added to its entry
+                                 (the subtree sizes the learned schedule trains on) */
 } gmk_opts;
 
 typedef struct {
@@ -121,6 +130,49 @@ void gmk_opts_default(gmk_opts* o);
  * Enumerates the maximal k-biplexes of g on its device. */
 int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
                   gmk_stats* out);
+
+/* No counterpart in the reference, which has no resume (its "checkpoints" are
+ * result-count milestones, src/main.cu:1753-1761).  Runs gmk_enumerate over
+ * consecutive batches of `batch_roots` roots (0 = automatic) and, after each
+ * batch, atomically rewrites `checkpoint_path` with the next root position
+ * and the running count and set hash.  If the file exists when the call
+ * starts, the run resumes from it (it must have been written for the same
+ * graph, k and schedule; else GMK_E_CHECKPOINT).  Results of finished batches
+ * are not delivered again.  With max_batches > 0 the call returns GMK_PAUSED
+ * after that many batches if work remains.  *out holds the totals of the
+ * whole run, resumed part included; a finished run leaves the file marked
+ * done. */
+int gmk_enumerate_resumable(gmk_graph* g, const gmk_opts* opts, const char* checkpoint_path,
+                            uint32_t batch_roots, uint32_t max_batches, gmk_sink sink,
+                            void* user, gmk_stats* out);
+
+/* ---- learned schedule: subtree-size model (no counterpart in the reference)
+ * A 16-64-64-1 ReLU perceptron with FP16 weights and inputs and FP32
+ * accumulation, trained and run on the GPU by the library's own kernels.  It
+ * predicts log1p(search nodes) of each root task from 16 integer-derived
+ * features; GMK_SCHEDULE_ORDERED then starts the largest predicted roots
+ * first.  It orders work only and never prunes. */
+typedef struct gmk_mlp gmk_mlp;
+#define GMK_MLP_FEATURES 16
+#define GMK_MLP_PARAMS 5313   /* W1[64][16] b1[64] W2[64][64] b2[64] W3[64] b3 */
+
+/* The 16 features of every root x in U (n_left x 16 floats, row-major), computed
+ * on the graph's device and rounded to FP16 as the model reads them. */
+int gmk_root_features(const gmk_graph* g, uint32_t k, float* out);
+
+/* A model on `device` with He-uniform weights drawn from `seed`. */
+int gmk_mlp_create(int device, uint64_t seed, gmk_mlp** out);
+void gmk_mlp_free(gmk_mlp* m);
+/* Copies the FP32 master weights out (get != NULL) and/or in (set != NULL). */
+int gmk_mlp_params(gmk_mlp* m, float* get, const float* set);
+/* Mean squared error of n samples and its gradient (GMK_MLP_PARAMS floats),
+ * without updating the weights. */
+int gmk_mlp_gradient(gmk_mlp* m, const float* x, const float* y, uint32_t n, float* grad,
+                     float* loss);
+/* `epochs` full-batch Adam steps on (x, y); *loss receives the last loss. */
+int gmk_mlp_train(gmk_mlp* m, const float* x, const float* y, uint32_t n, uint32_t epochs,
+                  float lr, float* loss);
+int gmk_mlp_predict(gmk_mlp* m, const float* x, uint32_t n, float* out);
 
 /* Canonical per-result hash pair (the set summary's h1/h2): ids are the
  * global ids of X u Y in any order, nx = |X|, ny = |Y|.  Host-only. */

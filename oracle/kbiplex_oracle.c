@@ -221,7 +221,15 @@ static void branch(ctx_t* c, const uint32_t* C, uint32_t nc, const uint32_t* E, 
 int oracle_enumerate(const uint32_t* offsets, const uint32_t* adj, uint32_t n,
                      uint32_t n_left, uint32_t k, uint64_t result_limit,
                      oracle_sink sink, void* user, oracle_stats* out) {
+    return oracle_enumerate_shard(offsets, adj, n, n_left, k, result_limit, 0, 1, sink, user, out);
+}
+
+int oracle_enumerate_shard(const uint32_t* offsets, const uint32_t* adj, uint32_t n,
+                           uint32_t n_left, uint32_t k, uint64_t result_limit,
+                           uint32_t shard, uint32_t nshards,
+                           oracle_sink sink, void* user, oracle_stats* out) {
     if (!offsets || !out || n > ORACLE_MAX_N || n_left > n || k < 1) return -1;
+    if (nshards == 0 || shard >= nshards) return -1;
     memset(out, 0, sizeof(*out));
     ctx_t c;
     memset(&c, 0, sizeof(c));
@@ -243,6 +251,7 @@ int oracle_enumerate(const uint32_t* offsets, const uint32_t* adj, uint32_t n,
     uint32_t* C = (uint32_t*)malloc((size_t)(n + 1) * sizeof(uint32_t));
     uint32_t* E = (uint32_t*)malloc((size_t)(n + 1) * sizeof(uint32_t));
     for (uint32_t x = 0; x < n_left && !c.stop; ++x) {
+        if (x % nshards != shard) continue;
         uint32_t nc = 0, ne = 0;
         for (uint32_t v = n_left; v < n; ++v) C[nc++] = v;        /* V first */
         for (uint32_t u = x + 1; u < n_left; ++u) C[nc++] = u;    /* later U */

@@ -35,6 +35,13 @@ int oracle_enumerate(const uint32_t* offsets, const uint32_t* adj, uint32_t n,
                      uint32_t n_left, uint32_t k, uint64_t result_limit,
                      oracle_sink sink, void* user, oracle_stats* out);
 
+/* Same, restricted to the roots x (smallest U vertex of a result) with
+ * x % nshards == shard: the shards partition the result set. */
+int oracle_enumerate_shard(const uint32_t* offsets, const uint32_t* adj, uint32_t n,
+                           uint32_t n_left, uint32_t k, uint64_t result_limit,
+                           uint32_t shard, uint32_t nshards,
+                           oracle_sink sink, void* user, oracle_stats* out);
+
 /* Canonical per-result hash pair of a vertex-id set (order-independent). */
 void oracle_result_hash(const uint32_t* ids, uint32_t n_ids, uint32_t nx,
                         uint32_t ny, uint64_t* h1, uint64_t* h2);

@@ -99,6 +99,11 @@ def _load():
             ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint32,
             ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, _SINK, ctypes.c_void_p,
             ctypes.POINTER(_Stats)]
+        lib.oracle_enumerate_shard.restype = ctypes.c_int
+        lib.oracle_enumerate_shard.argtypes = [
+            ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint32,
+            ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32,
+            _SINK, ctypes.c_void_p, ctypes.POINTER(_Stats)]
         lib.oracle_classify.restype = ctypes.c_int
         lib.oracle_classify.argtypes = [
             ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint32,
@@ -117,7 +122,10 @@ def _csr32(g):
     return off, adj, off.ctypes.data_as(P), adj.ctypes.data_as(P)
 
 
-def enumerate_oracle(g, k: int, result_limit: int = 0, collect: bool = False) -> OracleStats:
+def enumerate_oracle(g, k: int, result_limit: int = 0, collect: bool = False,
+                     shard: int = 0, nshards: int = 1) -> OracleStats:
+    """All maximal k-biplexes of g (or, with nshards > 1, those whose smallest U
+    vertex x has x % nshards == shard)."""
     lib = _load()
     off, adj, poff, padj = _csr32(g)
     out = []
@@ -129,8 +137,8 @@ def enumerate_oracle(g, k: int, result_limit: int = 0, collect: bool = False) ->
     else:
         cb = _SINK(0)
     st = _Stats()
-    rc = lib.oracle_enumerate(poff, padj, g.n, g.n_left, k, result_limit, cb, None,
-                              ctypes.byref(st))
+    rc = lib.oracle_enumerate_shard(poff, padj, g.n, g.n_left, k, result_limit, shard, nshards,
+                                    cb, None, ctypes.byref(st))
     if rc != 0:
         raise ValueError(f"oracle_enumerate failed ({rc}); n={g.n} (max 16384), k={k}")
     return OracleStats(st.count, st.hash_sum, st.hash_xor, st.nodes, bool(st.truncated),

@@ -1,0 +1,99 @@
+"""The learned schedule on the GPU: the MLP kernels' loss and gradients
+against the CPU float64 restatement (oracle/mlp_ref.py), training reduces the
+loss, the model ranks roots by subtree size on held-out graphs, and ordering
+by its predictions changes the schedule but never the result set."""
+import numpy as np
+import pytest
+
+import gmkbe_b200 as G
+from gmkbe_b200 import graphgen as gg
+from gmkbe_b200 import learned as L
+from oracle import mlp_ref
+from conftest import golden_graph_path
+
+pytestmark = pytest.mark.gpu
+
+# FP16 weights and inputs are the same on both sides; only the accumulation
+# differs (FP32 on the GPU, float64 here).  Tolerance: 1e-3 of the largest
+# gradient component, and 1e-4 relative on the loss.
+GRAD_RTOL = 1e-3
+LOSS_RTOL = 1e-4
+
+
+def _random_problem(seed, n):
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(0, 4, (n, 16)).astype(np.float32)
+    y = (0.5 * x[:, 2] + np.sin(x[:, 6]) + 0.1 * rng.standard_normal(n)).astype(np.float32)
+    return x, y
+
+
+@pytest.mark.parametrize("seed,n", [(1, 7), (2, 300), (3, 4096)])
+def test_gradient_matches_cpu_reference(seed, n):
+    m = L.SubtreeModel(seed=seed)
+    x, y = _random_problem(seed, n)
+    g_gpu, loss_gpu = m.gradient(x, y)
+    loss_cpu, g_cpu = mlp_ref.loss_and_gradient(m.params(), x, y)
+    assert abs(loss_gpu - loss_cpu) <= LOSS_RTOL * max(1.0, abs(loss_cpu))
+    scale = np.abs(g_cpu).max()
+    assert scale > 0
+    assert np.abs(g_gpu - g_cpu).max() <= GRAD_RTOL * scale
+
+
+def test_forward_matches_cpu_reference():
+    m = L.SubtreeModel(seed=9)
+    x, _ = _random_problem(9, 513)
+    got = m.predict(x)
+    want = mlp_ref.forward(m.params(), x)[0]
+    assert np.abs(got - want).max() <= 1e-4 * max(1.0, np.abs(want).max())
+
+
+def test_training_reduces_loss_and_learns_the_order():
+    m = L.SubtreeModel(seed=4)
+    x, y = _random_problem(5, 2000)
+    _, before = m.gradient(x, y)
+    after = m.train(x, y, epochs=300, lr=3e-3)
+    assert after < 0.25 * before
+    xt, yt = _random_problem(6, 500)
+    assert L.spearman(m.predict(xt), yt) > 0.8
+
+
+def _small_graphs(seeds):
+    return [gg.erdos_renyi(40, 40, 0.12, s) for s in seeds] + \
+           [gg.chung_lu(60, 120, 420, 2.1, s, max_deg=25) for s in seeds]
+
+
+def test_features_and_subtree_log_on_the_gpu():
+    g = gg.read_graph_bin(golden_graph_path("southernwomen"))
+    with G.Graph.from_graph(g) as dg:
+        f = L.root_features(dg, 1)
+        assert f.shape == (g.n_left, 16)
+        deg = g.degree()[: g.n_left]
+        assert np.allclose(f[:, 2], np.log1p(deg), atol=2e-3 * np.log1p(deg).max())
+        nodes = L.subtree_nodes(dg, 1)
+        total = dg.enumerate(k=1, schedule="plain")
+        assert nodes.sum() == total.nodes and (nodes > 0).all()
+
+
+def test_learned_order_ranks_roots_and_keeps_the_set():
+    k = 1
+    xs, ys = [], []
+    for g in _small_graphs(range(10, 20)):
+        with G.Graph.from_graph(g) as dg:
+            xs.append(L.root_features(dg, k))
+            ys.append(L.target(L.subtree_nodes(dg, k)))
+    model = L.SubtreeModel(seed=1)
+    model.train(np.concatenate(xs), np.concatenate(ys), epochs=600, lr=3e-3)
+    rhos = []
+    for g in _small_graphs([30, 31]):
+        with G.Graph.from_graph(g) as dg:
+            nodes = L.subtree_nodes(dg, k)
+            cost = L.predicted_costs(model, dg, k)
+            rhos.append(L.spearman(cost, nodes))
+            want = dg.enumerate(k=k, schedule="plain").summary()
+            assert dg.enumerate(k=k, schedule="ordered", task_cost=cost).summary() == want
+            # list-scheduling finish time with the measured costs: the learned
+            # order is never worse than id order by more than one task
+            ident = L.makespan(nodes, np.arange(g.n_left), 8)
+            lpt = L.makespan(nodes, np.argsort(-cost, kind="stable"), 8)
+            assert lpt <= ident + nodes.max()
+    assert np.mean(rhos) > 0.5

@@ -23,7 +23,7 @@ LIB_PATH = os.path.join(_PKG, "libgmk.so")
 # entry points declared in include/gmk.h
 EXPORTS = ("gmk_graph_load", "gmk_graph_from_csr", "gmk_graph_info", "gmk_graph_free",
            "gmk_opts_default", "gmk_enumerate", "gmk_enumerate_resumable",
-           "gmk_result_hash", "gmk_strerror", "gmk_last_cuda_error",
+           "gmk_enumerate_noalloc", "gmk_result_hash", "gmk_strerror", "gmk_last_cuda_error",
            "gmk_abi_version", "gmk_root_features", "gmk_mlp_create", "gmk_mlp_free",
            "gmk_mlp_params", "gmk_mlp_gradient", "gmk_mlp_train", "gmk_mlp_predict")
 
@@ -92,6 +92,10 @@ def load_library(path: str = LIB_PATH):
     lib.gmk_enumerate_resumable.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Opts), ctypes.c_char_p,
                                             ctypes.c_uint32, ctypes.c_uint32, SINK,
                                             ctypes.c_void_p, ctypes.POINTER(_Stats)]
+    lib.gmk_enumerate_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+                                          ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64,
+                                          ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                          ctypes.c_void_p, ctypes.POINTER(_Stats)]
     PF = ctypes.POINTER(ctypes.c_float)
     lib.gmk_root_features.argtypes = [ctypes.c_void_p, ctypes.c_uint32, PF]
     lib.gmk_mlp_create.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)]

@@ -371,6 +371,7 @@ const char* gmk_strerror(int code) {
         case GMK_E_SINK: return "stopped by the sink";
         case GMK_E_NODEV: return "no usable CUDA device";
         case GMK_E_CHECKPOINT: return "checkpoint unreadable or written for another graph / k";
+        case GMK_E_SCRATCH: return "request does not fit the static scratch (GMK_STATIC_SCRATCH_BYTES)";
         case GMK_PAUSED: return "paused (checkpoint written, work remains)";
         default: return "unknown error";
     }
@@ -876,6 +877,92 @@ int gmk_mlp_predict(gmk_mlp* m, const float* x, uint32_t n, float* out) {
     CK(cudaGetLastError());
     CK(cudaMemcpy(out, m->d_out, (uint64_t)n * sizeof(float), cudaMemcpyDeviceToHost));
     return GMK_OK;
+}
+
+namespace {
+
+// Scratch of gmk_enumerate_noalloc: counters, then the search arenas, then the
+// member buffers.  Host code must not use the symbol's host-side shadow as a
+// device address; noalloc_scratch() returns the real address per device.
+static __device__ __align__(256) unsigned char g_static_scratch[GMK_STATIC_SCRATCH_BYTES];
+
+std::mutex g_static_mu;
+void* g_static_addr[kMaxDevices] = {};
+
+// Device address of g_static_scratch on the current device (looked up once).
+int noalloc_scratch(int device, unsigned char** out) {
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_addr[device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_static_scratch)");
+        g_static_addr[device] = p;
+    }
+    *out = static_cast<unsigned char*>(g_static_addr[device]);
+    return GMK_OK;
+}
+
+}  // namespace
+
+int gmk_enumerate_noalloc(const uint32_t* d_offsets, const uint32_t* d_adj, uint32_t n,
+                          uint32_t n_left, uint32_t k, uint64_t result_limit, uint32_t threads,
+                          uint32_t arena_words, uint32_t max_members, void* stream,
+                          gmk_stats* out) {
+    if (!d_offsets || !out || (!d_adj && n > 0) || n_left > n) return GMK_E_INVAL;
+    if (k < 1 || k > 15) return GMK_E_INVAL;
+    std::memset(out, 0, sizeof(*out));
+    threads = threads ? threads : 2048u;
+    threads = (threads + kBlock - 1) / kBlock * kBlock;
+    arena_words = arena_words ? arena_words : 4096u;
+    max_members = max_members ? max_members : 512u;
+    const uint64_t need = 256ull + (uint64_t)threads * (4ull * arena_words + 8ull * max_members);
+    if (need > GMK_STATIC_SCRATCH_BYTES) return GMK_E_SCRATCH;
+    int device = 0;
+    CK(cudaGetDevice(&device));
+    if (device < 0 || device >= kMaxDevices) return GMK_E_INVAL;
+    if (n_left == 0 || n == n_left) return GMK_OK;   // a side is empty: no k-biplex
+    unsigned char* base = nullptr;
+    if (int rc = noalloc_scratch(device, &base)) return rc;
+    Counters* ctr = reinterpret_cast<Counters*>(base);
+    uint32_t* arenas = reinterpret_cast<uint32_t*>(base + 256);
+    uint32_t* sbuf = arenas + (uint64_t)threads * arena_words;
+    // tasks: root x with chunks of its first-level children, about 8 per thread
+    const uint32_t nv = n - n_left;
+    const uint64_t per_root = (8ull * threads + n_left - 1) / n_left;
+    uint32_t chunk = (uint32_t)std::max<uint64_t>(16, (nv + per_root - 1) / per_root);
+    chunk = std::min(chunk, nv);
+    const uint32_t chunks_per_root = (nv + chunk - 1) / chunk;
+    const unsigned long long n_tasks = (unsigned long long)n_left * chunks_per_root;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const auto t0 = std::chrono::steady_clock::now();
+    CK(cudaMemsetAsync(ctr, 0, sizeof(Counters), s));
+    gmk::GraphView gv{d_offsets, d_adj, n, n_left};
+    enumerate_kernel<<<threads / kBlock, kBlock, 0, s>>>(
+        gv, k, ctr, arenas, arena_words, sbuf, max_members, kDefaultPairLimit, n_tasks, chunk,
+        chunks_per_root, nullptr, 0u, result_limit, nullptr, 0ull, 0ull, 0u, 1u);
+    CK(cudaGetLastError());
+    Counters h;
+    CK(cudaMemcpyAsync(&h, ctr, sizeof(h), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    out->kernel_ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    out->count = result_limit ? std::min<unsigned long long>(h.count, result_limit) : h.count;
+    out->hash_sum = h.hash_sum;
+    out->hash_xor = h.hash_xor;
+    out->nodes = h.nodes;
+    out->algo_bytes = 4ull * h.work;
+    out->tasks = n_tasks;
+    out->tasks_done = std::min<unsigned long long>(h.tasks_done, n_tasks);
+    out->truncated = result_limit && h.count >= result_limit;
+    out->threads = threads;
+    out->rounds = 1;
+    switch (h.error) {
+        case gmk::TASK_OK: return GMK_OK;
+        case gmk::TASK_E_ARENA: return GMK_E_ARENA;
+        case gmk::TASK_E_SMAX: return GMK_E_SMAX;
+        case gmk::TASK_E_TIMEOUT: return GMK_E_TIMEOUT;
+        default: return GMK_E_CUDA;
+    }
 }
 
 namespace {

@@ -35,6 +35,7 @@ enum {
     GMK_E_SINK = -10,    /* the sink asked to stop (not an error for the caller's data) */
     GMK_E_NODEV = -11,   /* no CUDA device / extension not usable */
     GMK_E_CHECKPOINT = -12, /* checkpoint file unreadable, or written for another graph / k */
+    GMK_E_SCRATCH = -13, /* gmk_enumerate_noalloc: the request does not fit the static scratch */
     GMK_PAUSED = 1       /* not an error: max_batches reached, the checkpoint holds the rest */
 };
 
@@ -145,6 +146,37 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
 int gmk_enumerate_resumable(gmk_graph* g, const gmk_opts* opts, const char* checkpoint_path,
                             uint32_t batch_roots, uint32_t max_batches, gmk_sink sink,
                             void* user, gmk_stats* out);
+
+/* No counterpart in the reference.  An entry point for callers that must not
+ * allocate device memory: code running where cudaMalloc is unavailable or
+ * forbidden (inside a host allocator's own callbacks, under an external memory
+ * pool that owns all device memory, in a process that has pinned its device
+ * footprint before the search starts).  The caller passes the graph as device
+ * CSR arrays it owns (d_offsets: n+1 words, d_adj: d_offsets[n] words, rows
+ * sorted, U rows hold V ids and vice versa) and receives the counts and set
+ * hash in *out.  The search runs the one-task-per-thread engine with the batched
+ * schedule; its arenas, member buffers and counters live in one static device
+ * array of GMK_STATIC_SCRATCH_BYTES that every GPU loading libgmk.so holds until
+ * the process exits.  Nothing is allocated: no cudaMalloc, no cudaFree, no events.
+ *   threads:     search threads (0 = 2048), a multiple of 128 is used;
+ *   arena_words: per-thread search arena in u32 words (0 = 4096);
+ *   max_members: largest |X|+|Y| (0 = 512).
+ * threads x (4 arena_words + 8 max_members) bytes plus 256 for the counters must
+ * fit GMK_STATIC_SCRATCH_BYTES, else GMK_E_SCRATCH.  A search that outgrows its
+ * arena returns GMK_E_ARENA as gmk_enumerate does.
+ * The first call on a device looks up the array's device address (once per
+ * device, with that device made current); make that first call before any
+ * stream capture begins.  The call runs on `stream` (a cudaStream_t, NULL = the
+ * legacy default stream) and returns after the search finished.  All calls on a
+ * device share the one array, which keeps the last call's contents; each call
+ * clears the counters it needs.  Calls that overlap on the GPU (from several
+ * host threads or streams) race on the array and must be serialised by the
+ * caller.  out->kernel_ms is host wall time of the launch and wait. */
+#define GMK_STATIC_SCRATCH_BYTES (64u << 20)
+int gmk_enumerate_noalloc(const uint32_t* d_offsets, const uint32_t* d_adj, uint32_t n,
+                          uint32_t n_left, uint32_t k, uint64_t result_limit, uint32_t threads,
+                          uint32_t arena_words, uint32_t max_members, void* stream,
+                          gmk_stats* out);
 
 /* ---- learned schedule: subtree-size model (no counterpart in the reference)
  * A 16-64-64-1 ReLU perceptron with FP16 weights and inputs and FP32

@@ -18,10 +18,12 @@ from dataclasses import dataclass
 import numpy as np
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_PKG, "libgmk.so")
+# GMK_LIBRARY names another build of the library (for A/B measurements)
+LIB_PATH = os.environ.get("GMK_LIBRARY") or os.path.join(_PKG, "libgmk.so")
 
 # entry points declared in include/gmk.h
-EXPORTS = ("gmk_graph_load", "gmk_graph_from_csr", "gmk_graph_info", "gmk_graph_free",
+EXPORTS = ("gmk_graph_load", "gmk_graph_from_csr", "gmk_graph_info", "gmk_graph_fingerprint",
+           "gmk_graph_free",
            "gmk_opts_default", "gmk_enumerate", "gmk_enumerate_resumable",
            "gmk_enumerate_noalloc", "gmk_result_hash", "gmk_strerror", "gmk_last_cuda_error",
            "gmk_abi_version", "gmk_root_features", "gmk_mlp_create", "gmk_mlp_free",
@@ -83,6 +85,7 @@ def load_library(path: str = LIB_PATH):
     lib.gmk_graph_from_csr.argtypes = [P32, P32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int,
                                        ctypes.POINTER(ctypes.c_void_p)]
     lib.gmk_graph_info.argtypes = [ctypes.c_void_p, P32, P32, ctypes.POINTER(ctypes.c_uint64)]
+    lib.gmk_graph_fingerprint.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]
     lib.gmk_graph_free.argtypes = [ctypes.c_void_p]
     lib.gmk_graph_free.restype = None
     lib.gmk_opts_default.argtypes = [ctypes.POINTER(_Opts)]
@@ -160,6 +163,12 @@ class Graph:
         n, nl, m = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint64()
         _check(lib.gmk_graph_info(self._h, ctypes.byref(n), ctypes.byref(nl), ctypes.byref(m)))
         self.n, self.n_left, self.adj_len = n.value, nl.value, m.value
+
+    def fingerprint(self) -> int:
+        """64-bit hash of the CSR (the identity checkpoints and tuning caches record)."""
+        v = ctypes.c_uint64()
+        _check(load_library().gmk_graph_fingerprint(self._h, ctypes.byref(v)))
+        return v.value
 
     @classmethod
     def load(cls, path: str, device: int = 0) -> "Graph":
@@ -248,7 +257,7 @@ class Graph:
                   max_members: int = 0, watchdog_ms: int = 0, pair_limit: int = 0,
                   task_cost=None, sink=None, shard: int = 0, nshards: int = 1,
                   engine: str = "warp", split_min_nodes: int = 0, root_begin: int = 0,
-                  root_end: int = 0, root_nodes=None) -> Stats:
+                  root_end: int = 0, root_nodes=None, out_words: int = 0) -> Stats:
         """Enumerate maximal k-biplexes.  collect=True returns the result list
         (sorted X, Y tuples) in Stats.results; `sink(x, y)` is called per
         result otherwise (return True to stop).  root_nodes: a uint64 numpy
@@ -265,11 +274,14 @@ class Graph:
         out: list = []
         cb = self._sink(collect, sink, out)
         o.emit = 1 if (collect or sink is not None) else 0
+        o.out_words = out_words
         st = _Stats()
         while True:
             out.clear()
             rc = lib.gmk_enumerate(self._h, ctypes.byref(o), cb, None, ctypes.byref(st))
-            if rc != E_OUTBUF:
+            # a record buffer overflow is retried with a larger buffer only when
+            # no caller sink has seen results yet
+            if rc != E_OUTBUF or sink is not None:
                 break
             o.out_words = (o.out_words or (64 << 20)) * 4
         if rc != E_SINK:

@@ -129,6 +129,7 @@ enum : int {
     TASK_E_ARENA = 1,   // task arena too small
     TASK_E_SMAX = 2,    // |S| above the member capacity
     TASK_E_TIMEOUT = 3, // watchdog deadline passed
+    TASK_E_OUTBUF = 4,  // a result record found no room and could not be deferred
 };
 
 struct Outputs {
@@ -144,6 +145,7 @@ struct Outputs {
     unsigned long long* out_pos;
     unsigned long long out_cap;     // words
     unsigned long long deadline_ns; // 0 = none; compared with the device's global timer
+    unsigned long long* out_fail;   // warp engine: lowest record position that found no room
 };
 
 struct Task {

@@ -42,9 +42,16 @@ __device__ __forceinline__ unsigned long long edge_key(uint32_t a, uint32_t b) {
     return a < b ? ((unsigned long long)a << 32) | b : ((unsigned long long)b << 32) | a;
 }
 
+// Bucket of a key: a 32-bit multiply-xorshift mix of its two ids (the
+// multiplicative constants of the 32-bit golden-ratio / murmur3 finaliser
+// family), cheaper on the GPU than a 64-bit mix; buckets <= 2^32.
 __device__ __forceinline__ unsigned long long bucket_of(unsigned long long key,
                                                         unsigned long long bmask) {
-    return mix64(key) & bmask;
+    uint32_t h = (uint32_t)(key >> 32) * 0x9E3779B1u ^ (uint32_t)key * 0x85EBCA77u;
+    h ^= h >> 15;
+    h *= 0x2C1B3C6Du;
+    h ^= h >> 13;
+    return (unsigned long long)h & bmask;
 }
 
 __device__ __noinline__ bool has_edge_tail(const EdgeHash& h, unsigned long long key,
@@ -118,10 +125,23 @@ __device__ __forceinline__ T bcast(T v) { return __shfl_sync(kFull, v, 0); }
 struct SplitBuf {
     uint32_t* words;
     unsigned long long* idx;
-    unsigned long long* used;     // words reserved
-    unsigned long long* count;    // records reserved
+    int* refused;                 // first reason a split was refused (diagnostics; 0 = none)
+    unsigned long long* used;     // words reserved (may pass word_cap: those failed)
+    unsigned long long* count;    // records reserved (may pass idx_cap)
+    unsigned long long* count_fail;   // lowest record index whose reservation failed (~0: none)
     unsigned long long word_cap;
     unsigned long long idx_cap;
+};
+
+// Two per-side values.  Selected with a conditional, never indexed, so that
+// they stay in registers (an indexed 2-array would live in local memory).
+struct U2 {
+    uint32_t a, b;
+    __device__ __forceinline__ uint32_t get(int s) const { return s ? b : a; }
+    __device__ __forceinline__ void set(int s, uint32_t v) {
+        a = s ? a : v;
+        b = s ? v : b;
+    }
 };
 
 struct Ctx {
@@ -133,7 +153,8 @@ struct Ctx {
     uint32_t* sid;
     uint32_t* smc;
     uint32_t smax;
-    uint32_t ns, nss[2];
+    uint32_t ns;
+    U2 nss;                                      // |S| per side
     uint32_t scan_limit;
     int err;
     unsigned long long cnt, hsum, hxor, nodes;   // warp-uniform
@@ -182,7 +203,7 @@ __device__ void fail(Ctx& t, const Outputs& o, int code) {
 // (per lane; the same test as compat_misses in enum_core.cuh).
 __device__ uint32_t compat_lane(Ctx& t, uint32_t w) {
     const int s = side_of(t.g, w);
-    if (t.nss[1 - s] == 0) return 0;
+    if (t.nss.get(1 - s) == 0) return 0;
     uint32_t miss = 0;
     for (uint32_t i = 0; i < t.ns; ++i) {
         const uint32_t m = t.sid[i];
@@ -225,7 +246,7 @@ __device__ uint32_t push_member(Ctx& t, uint32_t c, uint32_t* nsat_out) {
     }
     __syncwarp();
     t.ns++;
-    t.nss[s]++;
+    t.nss.set(s, t.nss.get(s) + 1);
     if (nsat_out) *nsat_out = nsat < kSatCap ? nsat : kSatCap;
     return miss;
 }
@@ -234,7 +255,7 @@ __device__ void pop_member(Ctx& t) {
     const uint32_t c = t.sid[t.ns - 1];
     t.ns--;
     const int s = side_of(t.g, c);
-    t.nss[s]--;
+    t.nss.set(s, t.nss.get(s) - 1);
     for (uint32_t base = 0; base < t.ns; base += 32) {
         const uint32_t i = base + t.lane;
         if (i < t.ns) {
@@ -279,7 +300,7 @@ __device__ bool outsider_addable(Ctx& t, const uint32_t* l0, uint32_t n0, const 
         const uint32_t* lo = s ? l0 : l1;
         const uint32_t cs = s ? n1 : n0, co = s ? n0 : n1;
         const uint32_t* tots_o = tot + t.ns + (o ? n0 : 0);
-        const uint32_t nopp = t.nss[o] + co, nown = t.nss[s] + cs;
+        const uint32_t nopp = t.nss.get(o) + co, nown = t.nss.get(s) + cs;
         // the lowest-degree blocking member (tot >= k), S members first
         unsigned long long best = ~0ull;
         for (uint32_t base = 0; base < t.ns; base += 32) {
@@ -408,7 +429,7 @@ __device__ bool outsider_addable_mixed(Ctx& t, int s, uint32_t lo, const uint32_
         for (uint32_t j = t.lane; j < t.k + 1; j += 32) t.src[j] = j < nm ? mem[j] : l[2 * (j - nm)];
         nsrc = t.k + 1;
     } else {
-        return (lo + 1 - side_begin(g, s)) > t.nss[s];
+        return (lo + 1 - side_begin(g, s)) > t.nss.get(s);
     }
     __syncwarp();
     for (uint32_t q = 0; q < nsrc; ++q) {
@@ -449,7 +470,9 @@ __device__ bool outsider_addable_mixed(Ctx& t, int s, uint32_t lo, const uint32_
 
 // ----------------------------------------------------------------- emission
 
-__device__ void emit(Ctx& t, const Outputs& o, const uint32_t* l0, uint32_t n0, const uint32_t* l1,
+// Counts (and in record mode writes) the result S u list0 u list1.  Returns
+// false only in record mode when the record found no room.
+__device__ bool emit(Ctx& t, const Outputs& o, const uint32_t* l0, uint32_t n0, const uint32_t* l1,
                      uint32_t n1) {
     unsigned long long a = 0, b = 0;
     for (uint32_t i = t.lane; i < t.ns; i += 32) {
@@ -466,27 +489,40 @@ __device__ void emit(Ctx& t, const Outputs& o, const uint32_t* l0, uint32_t n0, 
     }
     a = warp_sum64(a);
     b = warp_sum64(b);
-    const uint32_t nx = t.nss[0] + n0, ny = t.nss[1] + n1;
+    const uint32_t nx = t.nss.a + n0, ny = t.nss.b + n1;
     if (o.out_buf) {
-        // record mode: one reservation per result, exact limit
+        // record mode: room first, then the count (exact limit).  A record
+        // that finds no room is not counted: the caller defers the node to
+        // the next round, after the host has drained the buffer.
         const unsigned long long words = 2ull + nx + ny;
-        unsigned long long c = 0, at = 0;
+        unsigned long long at = 0;
+        int room = 0, keep = 0;
         if (t.lane == 0) {
-            c = atomicAdd(o.count, 1ull);
-            if (!(o.limit && c >= o.limit)) {
-                if (o.limit && c + 1 >= o.limit) atomicExch(o.stop, 1);
-                atomicAdd(o.hash_sum, final_h1(a, nx, ny));
-                atomicXor(o.hash_xor, final_h2(b, nx, ny));
-                at = atomicAdd(o.out_pos, words);
+            at = atomicAdd(o.out_pos, words);
+            room = at + words <= o.out_cap;
+            if (!room) {
+                atomicMin(o.out_fail, at);
             } else {
-                atomicExch(o.stop, 1);
+                const unsigned long long c = atomicAdd(o.count, 1ull);
+                keep = !(o.limit && c >= o.limit);
+                if (o.limit && c + 1 >= o.limit) atomicExch(o.stop, 1);
+                if (keep) {
+                    atomicAdd(o.hash_sum, final_h1(a, nx, ny));
+                    atomicXor(o.hash_xor, final_h2(b, nx, ny));
+                }
             }
         }
-        c = bcast(c);
+        room = bcast(room);
+        keep = bcast(keep);
         at = bcast(at);
-        if (o.limit && c >= o.limit) return;
-        if (at + words > o.out_cap) return;   // the host sees out_pos > cap: overflow
+        if (!room) return false;
         uint32_t* r = o.out_buf + at;
+        if (!keep) {
+            // past the limit: a skip record of the same length
+            if (t.lane == 0) { r[0] = 0xFFFFFFFFu; r[1] = (uint32_t)(words - 2); }
+            __syncwarp();
+            return true;
+        }
         if (t.lane == 0) { r[0] = nx; r[1] = ny; }
         uint32_t px = 2, py = 2 + nx;
         for (uint32_t base = 0; base < t.ns; base += 32) {
@@ -503,26 +539,30 @@ __device__ void emit(Ctx& t, const Outputs& o, const uint32_t* l0, uint32_t n0, 
         }
         for (uint32_t i = t.lane; i < n0; i += 32) r[px + i] = l0[2 * i];
         for (uint32_t i = t.lane; i < n1; i += 32) r[py + i] = l1[2 * i];
-        return;
+        __syncwarp();
+        return true;
     }
     t.cnt++;
     t.hsum += final_h1(a, nx, ny);
     t.hxor ^= final_h2(b, nx, ny);
     if (t.cnt >= kFlushBatch) flush(t, o);
+    return true;
 }
 
 // ----------------------------------------------------------------- frames
 
 struct Hdr {
-    uint32_t ns, flags, lo[2], cnt[2], off[2], order, phase, pos, top, parent, end;
+    uint32_t ns, flags;
+    U2 lo, cnt, off;
+    uint32_t order, phase, pos, top, parent, end;
 };
 
 __device__ __forceinline__ Hdr read_hdr(const uint32_t* f) {
     Hdr h;
     h.ns = f[F_NS]; h.flags = f[F_FLAGS];
-    h.lo[0] = f[F_LO0]; h.lo[1] = f[F_LO1];
-    h.cnt[0] = f[F_CNT0]; h.cnt[1] = f[F_CNT1];
-    h.off[0] = f[F_OFF0]; h.off[1] = f[F_OFF1];
+    h.lo.a = f[F_LO0]; h.lo.b = f[F_LO1];
+    h.cnt.a = f[F_CNT0]; h.cnt.b = f[F_CNT1];
+    h.off.a = f[F_OFF0]; h.off.b = f[F_OFF1];
     h.order = f[F_ORDER]; h.phase = f[F_PHASE]; h.pos = f[F_POS];
     h.top = f[F_TOP]; h.parent = f[F_PARENT_SLOT]; h.end = f[F_END];
     return h;
@@ -530,9 +570,9 @@ __device__ __forceinline__ Hdr read_hdr(const uint32_t* f) {
 
 __device__ __forceinline__ void write_hdr(uint32_t* f, const Hdr& h) {
     f[F_NS] = h.ns; f[F_FLAGS] = h.flags;
-    f[F_LO0] = h.lo[0]; f[F_LO1] = h.lo[1];
-    f[F_CNT0] = h.cnt[0]; f[F_CNT1] = h.cnt[1];
-    f[F_OFF0] = h.off[0]; f[F_OFF1] = h.off[1];
+    f[F_LO0] = h.lo.a; f[F_LO1] = h.lo.b;
+    f[F_CNT0] = h.cnt.a; f[F_CNT1] = h.cnt.b;
+    f[F_OFF0] = h.off.a; f[F_OFF1] = h.off.b;
     f[F_ORDER] = h.order; f[F_PHASE] = h.phase; f[F_POS] = h.pos;
     f[F_TOP] = h.top; f[F_PARENT_SLOT] = h.parent; f[F_END] = h.end;
 }
@@ -568,16 +608,16 @@ __device__ uint32_t build_child(Ctx& t, const Outputs& o, uint32_t cur, uint32_t
     uint32_t w = nc + F_WORDS;
     if (w > t.cap) { fail(t, o, TASK_E_ARENA); return kNoPos; }
     Hdr ch;
-    ch.ns = t.ns; ch.flags = 0; ch.lo[0] = ch.lo[1] = 0; ch.cnt[0] = ch.cnt[1] = 0;
+    ch.ns = t.ns; ch.flags = 0; ch.lo.a = ch.lo.b = 0; ch.cnt.a = ch.cnt.b = 0; ch.off.a = ch.off.b = 0;
     ch.order = 0; ch.phase = 0; ch.pos = 0; ch.parent = cur; ch.end = 0xFFFFFFFFu;
 
     // ---- same side as c
-    ch.off[s] = w;
+    ch.off.set(s, w);
     uint32_t cnt = 0;
     if (f.flags & gbit(s)) {
         if (nsat == 0) {
             ch.flags |= gbit(s);
-            ch.lo[s] = c;
+            ch.lo.set(s, c);
         } else {
             uint32_t z = t.sat[0];
             for (uint32_t i = 1; i < nsat; ++i)
@@ -601,8 +641,8 @@ __device__ uint32_t build_child(Ctx& t, const Outputs& o, uint32_t cur, uint32_t
             }
         }
     } else {
-        const uint32_t* lst = t.arena + f.off[s];
-        const uint32_t n = f.cnt[s];
+        const uint32_t* lst = t.arena + f.off.get(s);
+        const uint32_t n = f.cnt.get(s);
         if (w + 2ull * n > t.cap) { fail(t, o, TASK_E_ARENA); return kNoPos; }
         const uint32_t start = forced ? 0u : p + 1;
         for (uint32_t base = start; base < n; base += 32) {
@@ -618,19 +658,19 @@ __device__ uint32_t build_child(Ctx& t, const Outputs& o, uint32_t cur, uint32_t
             append_pair(t, w, cnt, keep, v, m);
         }
     }
-    ch.cnt[s] = cnt;
+    ch.cnt.set(s, cnt);
     w += 2 * cnt;
 
     // ---- other side
-    ch.off[os] = w;
+    ch.off.set(os, w);
     cnt = 0;
     if (opp_done) {
         // that side was iterated first: nothing left on it
     } else if (f.flags & gbit(os)) {
-        const uint32_t lo = f.lo[os];
-        if (t.nss[s] <= t.k && mcc < t.k) {
+        const uint32_t lo = f.lo.get(os);
+        if (t.nss.get(s) <= t.k && mcc < t.k) {
             ch.flags |= gbit(os);
-            ch.lo[os] = lo;
+            ch.lo.set(os, lo);
         } else {
             // candidates touch c (saturated) or one of k+1 members of side s
             uint32_t nsrc;
@@ -669,8 +709,8 @@ __device__ uint32_t build_child(Ctx& t, const Outputs& o, uint32_t cur, uint32_t
             }
         }
     } else {
-        const uint32_t* lst = t.arena + f.off[os];
-        const uint32_t n = f.cnt[os];
+        const uint32_t* lst = t.arena + f.off.get(os);
+        const uint32_t n = f.cnt.get(os);
         if (w + 2ull * n > t.cap) { fail(t, o, TASK_E_ARENA); return kNoPos; }
         for (uint32_t base = 0; base < n; base += 32) {
             const uint32_t q = base + t.lane;
@@ -686,38 +726,49 @@ __device__ uint32_t build_child(Ctx& t, const Outputs& o, uint32_t cur, uint32_t
             append_pair(t, w, cnt, keep, v, m);
         }
     }
-    ch.cnt[os] = cnt;
+    ch.cnt.set(os, cnt);
     w += 2 * cnt;
     ch.top = w;
     for (int s2 = 0; s2 < 2; ++s2)
-        if ((ch.flags & gbit(s2)) && ch.lo[s2] + 1 >= side_end(g, s2)) {
+        if ((ch.flags & gbit(s2)) && ch.lo.get(s2) + 1 >= side_end(g, s2)) {
             ch.flags &= ~gbit(s2);
-            ch.cnt[s2] = 0;
+            ch.cnt.set(s2, 0);
         }
     if (t.lane == 0) write_hdr(t.arena + nc, ch);
     __syncwarp();
     return nc;
 }
 
-// Warp form of enter_node (enum_core.cuh).
-__device__ int enter_node(Ctx& t, const Outputs& o, uint32_t cur, uint32_t* next) {
+// enter_node: the node's result record found no room in the record buffer.
+constexpr int ENTER_DEFER = 3;
+
+// The child a node asks for: "S + c", c on side s at list position p.
+struct ChildReq {
+    uint32_t c, p;
+    int s;
+    bool forced, opp_done;
+};
+
+// Warp form of enter_node (enum_core.cuh).  ENTER_PUSHED: a forced candidate
+// was found; *req describes the child to build.
+__device__ int enter_node(Ctx& t, const Outputs& o, uint32_t cur, ChildReq* req) {
     const GraphView& g = t.g;
     const Hdr f = read_hdr(t.arena + cur);
     pop_to(t, f.ns);
     const bool g0 = f.flags & FL_G0, g1 = f.flags & FL_G1;
-    if (t.nss[1] == 0 && !g1 && f.cnt[1] == 0) return ENTER_DONE;   // Y must end up non-empty
+    if (t.nss.b == 0 && !g1 && f.cnt.b == 0) return ENTER_DONE;   // Y must end up non-empty
     if (g0 != g1) {
         const int s = g0 ? 0 : 1, os = 1 - s;
-        const uint32_t n = f.cnt[os];
+        const uint32_t n = f.cnt.get(os);
         const uint32_t base = f.top;
         if (base + n + 2ull * t.ns > t.cap) { fail(t, o, TASK_E_ARENA); return ENTER_DONE; }
-        if (outsider_addable_mixed(t, s, f.lo[s], t.arena + f.off[os], n, t.arena + base))
+        if (outsider_addable_mixed(t, s, f.lo.get(s), t.arena + f.off.get(os), n, t.arena + base))
             return ENTER_DONE;
     }
     if (!g0 && !g1) {
-        const uint32_t n0 = f.cnt[0], n1 = f.cnt[1];
-        const uint32_t* l0 = t.arena + f.off[0];
-        const uint32_t* l1 = t.arena + f.off[1];
+        const uint32_t n0 = f.cnt.a, n1 = f.cnt.b;
+        const uint32_t* l0 = t.arena + f.off.a;
+        const uint32_t* l1 = t.arena + f.off.b;
         const unsigned long long pairs = (unsigned long long)(t.ns + n0) * (t.ns + n1);
         if (n0 + n1 == 0 || pairs <= t.scan_limit) {
             const uint32_t base = f.top;
@@ -755,12 +806,14 @@ __device__ int enter_node(Ctx& t, const Outputs& o, uint32_t cur, uint32_t* next
             __syncwarp();
             bool bad = false;
             for (uint32_t i = t.lane; i < t.ns + n0 + n1; i += 32) bad |= tot[i] > t.k;
-            if (!__any_sync(kFull, bad)) {
+            const bool biplex = !__any_sync(kFull, bad);
+            const bool addable = outsider_addable(t, l0, n0, l1, n1, tot);
+            if (biplex) {
                 // S u C is a k-biplex: the only leaf that can be maximal
-                if (!outsider_addable(t, l0, n0, l1, n1, tot)) emit(t, o, l0, n0, l1, n1);
+                if (!addable && !emit(t, o, l0, n0, l1, n1)) return ENTER_DEFER;
                 return ENTER_DONE;
             }
-            if (outsider_addable(t, l0, n0, l1, n1, tot)) return ENTER_DONE;
+            if (addable) return ENTER_DONE;
             // forced candidate: fits every leaf that lacks it (first in list order)
             for (int s = 0; s < 2; ++s) {
                 const uint32_t* ls = s ? l1 : l0;
@@ -786,10 +839,11 @@ __device__ int enter_node(Ctx& t, const Outputs& o, uint32_t cur, uint32_t* next
                     const uint32_t mask = __ballot_sync(kFull, ok);
                     if (mask) {
                         const uint32_t qq = qbase + __ffs(mask) - 1;
-                        const uint32_t c = ls[2 * qq];
-                        const uint32_t chn = build_child(t, o, cur, c, s, qq, true, false);
-                        if (chn == kNoPos) return ENTER_DONE;
-                        *next = chn;
+                        req->c = ls[2 * qq];
+                        req->s = s;
+                        req->p = qq;
+                        req->forced = true;
+                        req->opp_done = false;
                         return ENTER_PUSHED;
                     }
                 }
@@ -800,20 +854,21 @@ __device__ int enter_node(Ctx& t, const Outputs& o, uint32_t cur, uint32_t* next
     uint32_t order;
     if (f.flags & FL_ROOT) order = 1u;   // the root branches on V first; root chunks rely on it
     else if (g0 != g1) order = g0 ? 1u : 0u;
-    else if (!g0) order = GMK_LOCAL_ORDER(f.cnt[0], f.cnt[1]);
+    else if (!g0) order = GMK_LOCAL_ORDER(f.cnt.a, f.cnt.b);
     else order = 1u;
     if (t.lane == 0) {
         uint32_t* fw = t.arena + cur;
         fw[F_ORDER] = order;
         fw[F_PHASE] = 0;
-        fw[F_POS] = (f.flags & gbit((int)order)) ? f.lo[order] + 1 : 0;
+        fw[F_POS] = (f.flags & gbit((int)order)) ? f.lo.get(order) + 1 : 0;
     }
     __syncwarp();
     return ENTER_ITERATE;
 }
 
-// Warp form of next_child (enum_core.cuh).
-__device__ uint32_t next_child(Ctx& t, const Outputs& o, uint32_t cur) {
+// Warp form of next_child (enum_core.cuh): advances frame cur to its next
+// child and describes it in *req; false when the frame is finished.
+__device__ bool next_child(Ctx& t, uint32_t cur, ChildReq* req) {
     const GraphView& g = t.g;
     uint32_t* f = t.arena + cur;
     const Hdr h = read_hdr(f);
@@ -826,9 +881,9 @@ __device__ uint32_t next_child(Ctx& t, const Outputs& o, uint32_t cur) {
         if (h.flags & gbit(s)) {
             const uint32_t end = phase == 0 && h.end < side_end(g, s) ? h.end : side_end(g, s);
             if (pos < end) { c = pos; p = kNoPos; ++pos; have = true; }
-        } else if (pos < h.cnt[s]) {
+        } else if (pos < h.cnt.get(s)) {
             p = pos;
-            c = t.arena[h.off[s] + 2 * p];
+            c = t.arena[h.off.get(s) + 2 * p];
             ++pos;
             have = true;
         }
@@ -843,17 +898,22 @@ __device__ uint32_t next_child(Ctx& t, const Outputs& o, uint32_t cur) {
             ++phase;
             if (phase == 1) {
                 const int s2 = 1 - (int)h.order;
-                pos = (h.flags & gbit(s2)) ? h.lo[s2] + 1 : 0;
+                pos = (h.flags & gbit(s2)) ? h.lo.get(s2) + 1 : 0;
             }
             continue;
         }
         if (t.lane == 0) { f[F_PHASE] = phase; f[F_POS] = pos; }
         __syncwarp();
-        return build_child(t, o, cur, c, s, p, false, opp_done);
+        req->c = c;
+        req->s = s;
+        req->p = p;
+        req->forced = false;
+        req->opp_done = opp_done;
+        return true;
     }
     if (t.lane == 0) { f[F_PHASE] = phase; f[F_POS] = pos; }
     __syncwarp();
-    return kNoPos;
+    return false;
 }
 
 // ----------------------------------------------------------------- splitting
@@ -871,20 +931,6 @@ __device__ __forceinline__ uint32_t frame_list_words(const uint32_t* f) {
     return 2 * (c0 + c1);
 }
 
-// Bounded CAS reservation of `want` units under `cap`; returns the start or
-// ~0ull when it does not fit.
-__device__ unsigned long long reserve(unsigned long long* ctr, unsigned long long want,
-                                      unsigned long long cap) {
-    unsigned long long cur = *(volatile unsigned long long*)ctr;
-    for (int tries = 0; tries < 64; ++tries) {
-        if (cur + want > cap) return ~0ull;
-        const unsigned long long prev = atomicCAS(ctr, cur, cur + want);
-        if (prev == cur) return cur;
-        cur = prev;
-    }
-    return ~0ull;
-}
-
 // Writes every pending frame on the path from `cur` to the root as a task of
 // the next round.  All-or-nothing: returns false (and writes nothing) when
 // the buffer cannot take them all.
@@ -894,19 +940,36 @@ __device__ bool split_path(Ctx& t, const SplitBuf& sb, uint32_t cur) {
     for (uint32_t x = cur; x != kNoPos; x = t.arena[x + F_PARENT_SLOT]) {
         const uint32_t* f = t.arena + x;
         if (!frame_pending(f, x == cur)) continue;
-        if ((f[F_FLAGS] & FL_ROOT) && !(f[F_FLAGS] & FL_ENTERED)) return false;
+        if ((f[F_FLAGS] & FL_ROOT) && !(f[F_FLAGS] & FL_ENTERED)) {
+            if (t.lane == 0) atomicCAS(sb.refused, 0, 1);
+            return false;
+        }
         words += 3ull + 2ull * f[F_NS] + F_WORDS + frame_list_words(f);
         ++recs;
     }
-    if (recs == 0) return false;
-    unsigned long long w0 = 0, r0 = 0;
-    if (t.lane == 0) {
-        w0 = reserve(sb.used, words, sb.word_cap);
-        r0 = w0 == ~0ull ? ~0ull : reserve(sb.count, recs, sb.idx_cap);
+    if (recs == 0) {
+        if (t.lane == 0) atomicCAS(sb.refused, 0, 2);
+        return false;
     }
+    // Reservations are plain atomic adds (thousands of warps split at once
+    // when a round winds down).  Positions only grow, so once one reservation
+    // fails every later one fails too: the records below count_fail are the
+    // complete, written ones.  A failed word reservation is simply unused.
+    unsigned long long w0 = 0, r0 = 0;
+    int ok = 0;
+    if (t.lane == 0) {
+        w0 = atomicAdd(sb.used, words);
+        if (w0 + words <= sb.word_cap) {
+            r0 = atomicAdd(sb.count, recs);
+            if (r0 + recs <= sb.idx_cap) ok = 1;
+            else { atomicMin(sb.count_fail, r0); atomicCAS(sb.refused, 0, 4); }
+        } else {
+            atomicCAS(sb.refused, 0, 3);
+        }
+    }
+    if (!bcast(ok)) return false;
     w0 = bcast(w0);
     r0 = bcast(r0);
-    if (w0 == ~0ull || r0 == ~0ull) return false;   // a failed word reservation is left unused
     unsigned long long wp = w0, rp = r0;
     for (uint32_t x = cur; x != kNoPos; x = t.arena[x + F_PARENT_SLOT]) {
         const uint32_t* f = t.arena + x;
@@ -935,10 +998,19 @@ __device__ bool split_path(Ctx& t, const SplitBuf& sb, uint32_t cur) {
 // ----------------------------------------------------------------- tasks
 
 struct RunLimits {
-    uint32_t split_min_nodes;           // 0: never split
+    uint32_t split_min_nodes;           // 0: never split for load balance
     const unsigned long long* queue;    // the round's queue head
     unsigned long long queue_len;       // entries this warp's round hands out
+    // record mode: once *out_pos passes drain_at the round winds down -- every
+    // task is split into the next round after one node, so the host can drain
+    // the record buffer (0 = no draining)
+    const unsigned long long* out_pos;
+    unsigned long long drain_at;
 };
+
+__device__ __forceinline__ bool draining(const RunLimits& lim) {
+    return lim.drain_at && *(volatile const unsigned long long*)lim.out_pos >= lim.drain_at;
+}
 
 // Depth-first search from the frame at arena offset 0; returns the nodes it
 // entered.
@@ -947,16 +1019,18 @@ __device__ unsigned long long run_dfs(Ctx& t, const Outputs& o, uint32_t first,
     uint32_t cur = 0;
     uint32_t polls = 0;
     unsigned long long task_nodes = 0;
-    bool may_split = lim.split_min_nodes != 0 && sb != nullptr;
+    bool may_split = sb != nullptr && (lim.split_min_nodes != 0 || lim.drain_at != 0);
     while (cur != kNoPos) {
         if (t.err) break;
-        if ((++polls & 63u) == 0) {
+        if ((++polls & 15u) == 0) {
             int stop = 0, late = 0, hungry = 0;
             if (t.lane == 0) {
                 stop = load_flag(o.stop);
                 late = o.deadline_ns && now_ns() > o.deadline_ns;
-                hungry = may_split && task_nodes >= lim.split_min_nodes &&
-                         *(volatile const unsigned long long*)lim.queue >= lim.queue_len;
+                hungry = may_split && task_nodes >= 1 &&
+                         ((lim.split_min_nodes && task_nodes >= lim.split_min_nodes &&
+                           *(volatile const unsigned long long*)lim.queue >= lim.queue_len) ||
+                          draining(lim));
             }
             stop = bcast(stop); late = bcast(late); hungry = bcast(hungry);
             if (stop) break;
@@ -968,23 +1042,36 @@ __device__ unsigned long long run_dfs(Ctx& t, const Outputs& o, uint32_t first,
         }
         uint32_t* f = t.arena + cur;
         const uint32_t flags = f[F_FLAGS];
+        ChildReq req;
+        bool want = false;
         if (!(flags & FL_ENTERED)) {
             if (t.lane == 0) f[F_FLAGS] = flags | FL_ENTERED;
             __syncwarp();
             t.nodes++;
             task_nodes++;
-            uint32_t nxt = kNoPos;
-            const int r = enter_node(t, o, cur, &nxt);
-            if (r == ENTER_PUSHED) { set_word(t, cur + F_PHASE, 2); cur = nxt; continue; }
+            const int r = enter_node(t, o, cur, &req);
+            if (r == ENTER_DEFER) {
+                // re-enter this node next round, after the host drained the buffer
+                set_word(t, cur + F_FLAGS, flags);
+                t.nodes--;
+                task_nodes--;
+                if (sb && split_path(t, *sb, cur)) break;
+                fail(t, o, TASK_E_OUTBUF);
+                break;
+            }
             if (r == ENTER_DONE) { set_word(t, cur + F_PHASE, 2); cur = f[F_PARENT_SLOT]; continue; }
-            if ((flags & FL_ROOT) && f[F_ORDER] == 1u && (f[F_FLAGS] & FL_G1)) {
+            if (r == ENTER_PUSHED) {
+                set_word(t, cur + F_PHASE, 2);   // the forced child is its only child
+                want = true;
+            } else if ((flags & FL_ROOT) && f[F_ORDER] == 1u && (f[F_FLAGS] & FL_G1)) {
                 const uint32_t p = f[F_POS];
                 set_word(t, cur + F_POS, first > p ? first : p);
             }
         }
-        const uint32_t ch = next_child(t, o, cur);
-        if (ch == kNoPos) { cur = f[F_PARENT_SLOT]; continue; }
-        cur = ch;
+        if (!want) want = next_child(t, cur, &req);
+        if (!want) { cur = f[F_PARENT_SLOT]; continue; }
+        const uint32_t ch = build_child(t, o, cur, req.c, req.s, req.p, req.forced, req.opp_done);
+        cur = ch == kNoPos ? f[F_PARENT_SLOT] : ch;   // kNoPos: t.err is set, the loop ends
     }
     pop_to(t, 0);
     return task_nodes;
@@ -993,19 +1080,19 @@ __device__ unsigned long long run_dfs(Ctx& t, const Outputs& o, uint32_t first,
 // Root task: x in U with its first-level children y in [first, last).
 __device__ unsigned long long run_root(Ctx& t, const Outputs& o, uint32_t root, uint32_t first,
                                        uint32_t last, const SplitBuf* sb, const RunLimits& lim) {
-    t.ns = 0; t.nss[0] = t.nss[1] = 0;
+    t.ns = 0; t.nss.a = t.nss.b = 0;
     push_member(t, root, nullptr);
     Hdr h;
     h.ns = 1; h.flags = FL_G0 | FL_G1 | FL_ROOT;
-    h.lo[0] = root; h.lo[1] = t.g.nl - 1;
-    h.cnt[0] = h.cnt[1] = 0;
-    h.off[0] = h.off[1] = F_WORDS;
+    h.lo.a = root; h.lo.b = t.g.nl - 1;
+    h.cnt.a = h.cnt.b = 0;
+    h.off.a = h.off.b = F_WORDS;
     h.order = 0; h.phase = 0; h.pos = 0;
     h.top = F_WORDS; h.parent = kNoPos; h.end = last;
     for (int s = 0; s < 2; ++s)
-        if ((h.flags & gbit(s)) && h.lo[s] + 1 >= side_end(t.g, s)) {
+        if ((h.flags & gbit(s)) && h.lo.get(s) + 1 >= side_end(t.g, s)) {
             h.flags &= ~gbit(s);
-            h.cnt[s] = 0;
+            h.cnt.set(s, 0);
         }
     if (t.lane == 0) write_hdr(t.arena, h);
     __syncwarp();
@@ -1030,11 +1117,11 @@ __device__ unsigned long long run_record(Ctx& t, const Outputs& o, const uint32_
         }
         nv += __popc(__ballot_sync(kFull, isv));
     }
-    t.ns = ns; t.nss[1] = nv; t.nss[0] = ns - nv;
+    t.ns = ns; t.nss.b = nv; t.nss.a = ns - nv;
     const uint32_t* fr = r + 3 + 2 * ns;
     Hdr h = read_hdr(fr);
-    h.off[0] = F_WORDS;
-    h.off[1] = F_WORDS + 2 * c0;
+    h.off.a = F_WORDS;
+    h.off.b = F_WORDS + 2 * c0;
     h.top = F_WORDS + 2 * (c0 + c1);
     h.parent = kNoPos;
     const uint32_t* lr = fr + F_WORDS;

@@ -49,9 +49,13 @@ struct Counters {
     unsigned long long t0_ns;   // device clock at the first task (watchdog origin)
 };
 
-// Per-round queue and split-buffer counters of the warp engine.
+// Per-round queue, split-buffer and record-buffer counters of the warp engine.
 struct RoundCounters {
-    unsigned long long next_task, tasks_done, next_used, next_count;
+    unsigned long long next_task, tasks_done, next_used, next_count, out_pos;
+    unsigned long long out_fail;    // lowest record position that found no room (~0: none)
+    unsigned long long next_fail;   // lowest split-record index that found no room (~0: none)
+    int split_refused;              // first reason a split was refused (0 = none)
+    int pad;
 };
 
 constexpr int kBlock = 128;
@@ -71,6 +75,7 @@ enumerate_kernel(gmk::GraphView g, uint32_t k, Counters* ctr, uint32_t* arenas,
     o.count = &ctr->count; o.hash_sum = &ctr->hash_sum; o.hash_xor = &ctr->hash_xor;
     o.nodes = &ctr->nodes; o.work = &ctr->work; o.stop = &ctr->stop; o.error = &ctr->error;
     o.limit = limit; o.out_buf = out_buf; o.out_pos = &ctr->out_pos; o.out_cap = out_cap;
+    o.out_fail = nullptr;
     o.deadline_ns = watchdog_ns ? gmk::now_ns() + watchdog_ns : 0ull;
     gmk::Task t;
     t.g = g; t.k = k;
@@ -99,6 +104,12 @@ enumerate_kernel(gmk::GraphView g, uint32_t k, Counters* ctr, uint32_t* arenas,
 
 constexpr int kWBlock = 128;                 // 4 warps per block
 constexpr int kWarpsPerBlock = kWBlock / 32;
+// Resident blocks per SM the register allocation targets.  5 blocks (20 warps
+// per SM) leaves 96 registers a thread and no spills; measured faster on B200
+// than 32 warps per SM at 64 registers with spills.
+#ifndef GMK_WARP_MIN_BLOCKS
+#define GMK_WARP_MIN_BLOCKS 5
+#endif
 constexpr uint32_t kDefaultWarpArena = 1u << 18;
 
 struct WarpArgs {
@@ -112,13 +123,17 @@ struct WarpArgs {
     uint32_t* sbuf;
     uint32_t smax;
     uint32_t pair_limit;
-    int round;                         // 0: root tasks; > 0: split records
-    unsigned long long n_tasks;        // root tasks (round 0)
-    unsigned long long queue_len;      // queue entries this launch hands out
+    // the round's queue: entries [0, n_records) are split records, the rest
+    // root tasks root_task_base, root_task_base + 1, ... (this shard's numbering)
+    unsigned long long n_records;
+    unsigned long long root_task_base;
+    unsigned long long queue_len;
+    unsigned long long drain_at;       // record mode: wind the round down past this out_pos
     uint32_t chunk, chunks_per_root;
     const uint32_t* root_order;
     uint32_t root_base;                // first root position of this call
-    const uint32_t* cur_words;         // round > 0: records
+    uint32_t n_roots;                  // roots in this call
+    const uint32_t* cur_words;         // split records of the previous round
     const unsigned long long* cur_idx;
     gmk::warp::SplitBuf next;
     uint32_t split_min_nodes;          // 0: never split
@@ -130,7 +145,7 @@ struct WarpArgs {
     unsigned long long* root_nodes;    // optional per-root node log
 };
 
-__global__ void __launch_bounds__(kWBlock) enumerate_warp_kernel(const WarpArgs a) {
+__global__ void __launch_bounds__(kWBlock, GMK_WARP_MIN_BLOCKS) enumerate_warp_kernel(const WarpArgs a) {
     __shared__ uint32_t s_sat[kWarpsPerBlock][gmk::kSatCap];
     __shared__ uint32_t s_src[kWarpsPerBlock][gmk::warp::kSrcCap];
     using namespace gmk::warp;
@@ -141,7 +156,8 @@ __global__ void __launch_bounds__(kWBlock) enumerate_warp_kernel(const WarpArgs 
     gmk::Outputs o;
     o.count = &ctr->count; o.hash_sum = &ctr->hash_sum; o.hash_xor = &ctr->hash_xor;
     o.nodes = &ctr->nodes; o.work = &ctr->work; o.stop = &ctr->stop; o.error = &ctr->error;
-    o.limit = a.limit; o.out_buf = a.out_buf; o.out_pos = &ctr->out_pos; o.out_cap = a.out_cap;
+    o.limit = a.limit; o.out_buf = a.out_buf; o.out_pos = &a.rc->out_pos; o.out_cap = a.out_cap;
+    o.out_fail = &a.rc->out_fail;
     o.deadline_ns = 0;
     if (a.watchdog_ns) {
         // the first warp of the first round fixes the origin of the watchdog
@@ -157,7 +173,7 @@ __global__ void __launch_bounds__(kWBlock) enumerate_warp_kernel(const WarpArgs 
     t.g = a.g; t.eh = a.eh; t.k = a.k;
     t.arena = a.arenas + wid * a.arena_words; t.cap = a.arena_words;
     t.sid = a.sbuf + wid * 2ull * a.smax; t.smc = t.sid + a.smax; t.smax = a.smax;
-    t.ns = 0; t.nss[0] = t.nss[1] = 0;
+    t.ns = 0; t.nss.a = t.nss.b = 0;
     t.scan_limit = a.pair_limit; t.err = 0;
     t.cnt = t.hsum = t.hxor = t.nodes = 0; t.work = 0;
     t.sat = s_sat[wib]; t.src = s_src[wib]; t.lane = lane;
@@ -165,22 +181,43 @@ __global__ void __launch_bounds__(kWBlock) enumerate_warp_kernel(const WarpArgs 
     lim.split_min_nodes = a.split_min_nodes;
     lim.queue = &a.rc->next_task;
     lim.queue_len = a.queue_len;
-    const SplitBuf* sb = a.split_min_nodes ? &a.next : nullptr;
+    lim.out_pos = &a.rc->out_pos;
+    lim.drain_at = a.drain_at;
+    const SplitBuf* sb = (a.split_min_nodes || a.drain_at) ? &a.next : nullptr;
     for (;;) {
-        unsigned long long j = 0;
+        unsigned long long j = ~0ull;
         int stop = 0;
         if (lane == 0) {
             stop = gmk::load_flag(o.stop);
-            if (!stop) j = atomicAdd(&a.rc->next_task, 1ull);
+            if (!stop) {
+                if (!draining(lim)) {
+                    j = atomicAdd(&a.rc->next_task, 1ull);
+                } else {
+                    // winding down: take only split records (they must all be
+                    // taken, to be split again), leave the root tasks queued
+                    unsigned long long h = *(volatile unsigned long long*)&a.rc->next_task;
+                    for (int tries = 0; tries < (1 << 20) && h < a.n_records; ++tries) {
+                        const unsigned long long prev = atomicCAS(&a.rc->next_task, h, h + 1);
+                        if (prev == h) { j = h; break; }
+                        h = prev;
+                    }
+                    if (j == ~0ull && h < a.n_records) {
+                        atomicCAS(o.error, 0, gmk::TASK_E_TIMEOUT);
+                        atomicExch(o.stop, 1);
+                    }
+                }
+            }
         }
         stop = bcast(stop);
         j = bcast(j);
         if (stop || j >= a.queue_len) break;
         if (lane == 0) atomicAdd(&a.rc->tasks_done, 1ull);
-        if (a.round == 0) {
-            const unsigned long long id = j * a.nshards + a.shard;
-            const uint32_t r = a.root_base + (uint32_t)(id / a.chunks_per_root);
-            const uint32_t c = (uint32_t)(id % a.chunks_per_root);
+        if (j >= a.n_records) {
+            // chunk-major: every root's first chunk of children, then every
+            // root's second, ... (the low-degree V children come first)
+            const unsigned long long id = (a.root_task_base + (j - a.n_records)) * a.nshards + a.shard;
+            const uint32_t r = a.root_base + (uint32_t)(id % a.n_roots);
+            const uint32_t c = (uint32_t)(id / a.n_roots);
             const uint32_t root = a.root_order ? a.root_order[r] : r;
             const uint32_t first = a.g.nl + c * a.chunk;
             const unsigned long long end = (unsigned long long)first + a.chunk;
@@ -198,6 +235,32 @@ __global__ void __launch_bounds__(kWBlock) enumerate_warp_kernel(const WarpArgs 
     flush(t, o);
 }
 
+// CSR check on the device, one thread per vertex: offsets non-decreasing and
+// within adj, rows strictly ascending and holding ids of the other side only.
+// Also folds the CSR into an order-dependent 64-bit sum (the graph's
+// fingerprint, used to match checkpoints to graphs).
+__global__ void csr_check_kernel(const uint32_t* off, const uint32_t* adj, uint32_t n, uint32_t nl,
+                                 unsigned long long adj_len, int* bad, unsigned long long* fp) {
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const uint32_t a = off[v], b = off[v + 1];
+    unsigned long long h = gmk::mix64(((unsigned long long)v << 32 | a) ^ 0x6A09E667F3BCC909ull);
+    if (a > b || b > adj_len) {
+        atomicExch(bad, 1);
+        return;
+    }
+    const uint32_t lo = v < nl ? nl : 0u, hi = v < nl ? n : nl;
+    for (uint32_t p = a; p < b; ++p) {
+        const uint32_t w = adj[p];
+        if (w < lo || w >= hi || (p > a && adj[p - 1] >= w)) {
+            atomicExch(bad, 1);
+            return;
+        }
+        h += gmk::mix64(((unsigned long long)p << 32 | w) ^ 0xBB67AE8584CAA73Bull);
+    }
+    atomicAdd(fp, h);
+}
+
 bool read_file(const char* path, std::vector<uint32_t>& words) {
     FILE* fp = std::fopen(path, "rb");
     if (!fp) return false;
@@ -211,21 +274,6 @@ bool read_file(const char* path, std::vector<uint32_t>& words) {
     return got == words.size();
 }
 
-// Rows must be strictly ascending and hold ids of the other side only.
-int validate_csr(const uint32_t* off, const uint32_t* adj, uint32_t n, uint32_t nl) {
-    if (nl > n || off[0] != 0) return GMK_E_FORMAT;
-    for (uint32_t v = 0; v < n; ++v) {
-        if (off[v + 1] < off[v]) return GMK_E_FORMAT;
-        const uint32_t lo = v < nl ? nl : 0u, hi = v < nl ? n : nl;
-        for (uint32_t p = off[v]; p < off[v + 1]; ++p) {
-            const uint32_t w = adj[p];
-            if (w < lo || w >= hi) return GMK_E_FORMAT;
-            if (p > off[v] && adj[p - 1] >= w) return GMK_E_FORMAT;
-        }
-    }
-    return GMK_OK;
-}
-
 }  // namespace
 
 struct gmk_graph {
@@ -233,6 +281,7 @@ struct gmk_graph {
     uint32_t n = 0, nl = 0;
     uint64_t adj_len = 0;
     uint64_t fingerprint = 0;   // hash of the CSR (checkpoint identity)
+    uint32_t max_degree = 0;
     uint32_t* d_off = nullptr;
     uint32_t* d_adj = nullptr;
     Counters* d_ctr = nullptr;
@@ -244,6 +293,7 @@ struct gmk_graph {
     __half* d_feat = nullptr;                     // root features (on demand)
     RoundCounters* d_rc = nullptr;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;   // record delivery, overlapping the next round
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
@@ -269,6 +319,13 @@ struct Workspace {
 constexpr int kMaxDevices = 64;
 Workspace g_ws[kMaxDevices];
 
+// Per-device launch facts, looked up once (under the workspace mutex).
+struct DeviceInfo {
+    bool ready = false;
+    int sms = 0, per_sm_warp = 0, per_sm_thread = 0;
+};
+DeviceInfo g_dev[kMaxDevices];
+
 }  // namespace
 
 namespace {
@@ -284,10 +341,15 @@ int grow(void** p, size_t* have, size_t need) {
     return GMK_OK;
 }
 
+// Copies `words` record words from the device and hands every record to the
+// sink (ids sorted per side).  Runs on the graph's copy stream, so it overlaps
+// the round the enumeration stream is running.
+int deliver_records(gmk_graph* g, const uint32_t* d_rec, unsigned long long words, gmk_sink sink,
+                    void* user);
+
 int upload(const uint32_t* off, const uint32_t* adj, uint32_t n, uint32_t nl, int device,
            gmk_graph** out) {
-    int rc = validate_csr(off, adj, n, nl);
-    if (rc) return rc;
+    if (nl > n || off[0] != 0) return GMK_E_FORMAT;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         g_cuda_err = "no CUDA device";
@@ -298,15 +360,12 @@ int upload(const uint32_t* off, const uint32_t* adj, uint32_t n, uint32_t nl, in
     gmk_graph* g = new (std::nothrow) gmk_graph();
     if (!g) return GMK_E_NOMEM;
     g->device = device; g->n = n; g->nl = nl; g->adj_len = off[n];
-    {
-        uint64_t h = gmk::mix64(((uint64_t)n << 32) | nl);
-        for (uint32_t v = 0; v <= n; ++v) h = gmk::mix64(h ^ off[v]);
-        for (uint64_t p = 0; p < g->adj_len; ++p) h = gmk::mix64(h ^ adj[p]);
-        g->fingerprint = h;
-    }
+    for (uint32_t v = 0; v < n; ++v)
+        if (off[v + 1] > off[v]) g->max_degree = std::max(g->max_degree, off[v + 1] - off[v]);
     auto bail = [&](int code) { gmk_graph_free(g); return code; };
     cudaError_t e;
-    if ((e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking)) != cudaSuccess)
+    if ((e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&g->copy_stream, cudaStreamNonBlocking)) != cudaSuccess)
         return bail(cuda_fail(e, "cudaStreamCreate"));
     if ((e = cudaEventCreate(&g->ev0)) != cudaSuccess || (e = cudaEventCreate(&g->ev1)) != cudaSuccess)
         return bail(cuda_fail(e, "cudaEventCreate"));
@@ -324,6 +383,23 @@ int upload(const uint32_t* off, const uint32_t* adj, uint32_t n, uint32_t nl, in
         return bail(cuda_fail(e, "cudaMalloc(counters)"));
     if ((e = cudaMalloc(&g->d_rc, sizeof(RoundCounters))) != cudaSuccess)
         return bail(cuda_fail(e, "cudaMalloc(round counters)"));
+    // check the CSR on the device before anything reads it as a graph
+    {
+        struct Check { int bad; int pad; unsigned long long fp; } hc;
+        Check* dc = reinterpret_cast<Check*>(g->d_rc);   // scratch until the first enumeration
+        if ((e = cudaMemsetAsync(dc, 0, sizeof(Check), g->stream)) != cudaSuccess)
+            return bail(cuda_fail(e, "memset(check)"));
+        if (n) {
+            csr_check_kernel<<<(n + 255) / 256, 256, 0, g->stream>>>(g->d_off, g->d_adj, n, nl,
+                                                                     g->adj_len, &dc->bad, &dc->fp);
+            if ((e = cudaGetLastError()) != cudaSuccess) return bail(cuda_fail(e, "csr_check"));
+        }
+        if ((e = cudaMemcpyAsync(&hc, dc, sizeof(hc), cudaMemcpyDeviceToHost, g->stream)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(g->stream)) != cudaSuccess)
+            return bail(cuda_fail(e, "csr_check read-back"));
+        if (hc.bad) return bail(GMK_E_FORMAT);
+        g->fingerprint = gmk::mix64(hc.fp ^ (((uint64_t)n << 32) | nl));
+    }
     // edge hash: at most two keys per four slots
     {
         const unsigned long long edges = off[nl];
@@ -345,6 +421,31 @@ int upload(const uint32_t* off, const uint32_t* adj, uint32_t n, uint32_t nl, in
     }
     if ((e = cudaStreamSynchronize(g->stream)) != cudaSuccess) return bail(cuda_fail(e, "upload"));
     *out = g;
+    return GMK_OK;
+}
+
+}  // namespace
+
+namespace {
+
+int deliver_records(gmk_graph* g, const uint32_t* d_rec, unsigned long long words, gmk_sink sink,
+                    void* user) {
+    if (!words) return GMK_OK;
+    std::vector<uint32_t> rec(words);
+    CK(cudaMemcpyAsync(rec.data(), d_rec, 4ull * words, cudaMemcpyDeviceToHost, g->copy_stream));
+    CK(cudaStreamSynchronize(g->copy_stream));
+    size_t p = 0;
+    while (p + 2 <= rec.size()) {
+        const uint32_t nx = rec[p], ny = rec[p + 1];
+        if (nx == 0xFFFFFFFFu) { p += 2ull + ny; continue; }   // past the result limit
+        if (p + 2ull + nx + ny > rec.size()) break;
+        uint32_t* x = rec.data() + p + 2;
+        uint32_t* y = x + nx;
+        std::sort(x, x + nx);
+        std::sort(y, y + ny);
+        if (sink(user, x, nx, y, ny)) return GMK_E_SINK;
+        p += 2ull + nx + ny;
+    }
     return GMK_OK;
 }
 
@@ -430,6 +531,12 @@ int gmk_graph_info(const gmk_graph* g, uint32_t* n, uint32_t* n_left, uint64_t* 
     return GMK_OK;
 }
 
+int gmk_graph_fingerprint(const gmk_graph* g, uint64_t* out) {
+    if (!g || !out) return GMK_E_INVAL;
+    *out = g->fingerprint;
+    return GMK_OK;
+}
+
 void gmk_graph_free(gmk_graph* g) {
     if (!g) return;
     cudaSetDevice(g->device);
@@ -439,6 +546,7 @@ void gmk_graph_free(gmk_graph* g) {
     if (g->ev0) cudaEventDestroy(g->ev0);
     if (g->ev1) cudaEventDestroy(g->ev1);
     if (g->stream) cudaStreamDestroy(g->stream);
+    if (g->copy_stream) cudaStreamDestroy(g->copy_stream);
     delete g;
 }
 
@@ -467,33 +575,49 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
     if (g->nl == 0 || g->n == g->nl || root_begin == root_end) return GMK_OK;   // nothing to do
 
     const bool warp = opts->engine == GMK_ENGINE_WARP;
-    cudaDeviceProp prop;
-    CK(cudaGetDeviceProperties(&prop, g->device));
-    int per_sm = 0;
-    if (warp)
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, enumerate_warp_kernel, kWBlock, 0));
-    else
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, enumerate_kernel, kBlock, 0));
-    per_sm = std::max(per_sm, 1);
-    const int block = warp ? kWBlock : kBlock;
-    const uint32_t lanes_per_worker = warp ? 32u : 1u;
-    const uint32_t arena_words =
-        opts->arena_words ? opts->arena_words : (warp ? kDefaultWarpArena : kDefaultArena);
-    const uint32_t smax = opts->max_members ? opts->max_members : kDefaultSmax;
-    // workers: threads (thread engine) or warps (warp engine)
-    uint64_t threads = opts->threads ? opts->threads
-                                     : (uint64_t)prop.multiProcessorCount * per_sm * block;
-    threads = std::max<uint64_t>(threads, (uint64_t)block);
-    // keep the search arenas within 40% of free device memory
-    size_t free_b = 0, total_b = 0;
-    CK(cudaMemGetInfo(&free_b, &total_b));
-    const uint64_t per_worker = 4ull * arena_words + 8ull * smax;
     Workspace& ws = g_ws[g->device];
     std::lock_guard<std::mutex> lock(ws.mu);
-    const uint64_t budget = (uint64_t)((double)(free_b + ws.arena_bytes + ws.sbuf_bytes) * 0.4);
+    DeviceInfo& di = g_dev[g->device];
+    if (!di.ready) {
+        int sms = 0;
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&di.per_sm_warp, enumerate_warp_kernel,
+                                                         kWBlock, 0));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&di.per_sm_thread, enumerate_kernel,
+                                                         kBlock, 0));
+        di.sms = sms;
+        di.ready = true;
+    }
+    const int per_sm = std::max(warp ? di.per_sm_warp : di.per_sm_thread, 1);
+    const int block = warp ? kWBlock : kBlock;
+    const uint32_t lanes_per_worker = warp ? 32u : 1u;
+    // A warp's arena holds its stack of child lists: a list gathered from a hub's
+    // row is up to 2 deg words, and nested lists shrink; (k + 2) such lists
+    // per warp cover the depths seen on power-law graphs.
+    uint32_t arena_words = opts->arena_words;
+    if (!arena_words) {
+        arena_words = warp ? kDefaultWarpArena : kDefaultArena;
+        if (warp) {
+            const uint64_t hub = 2ull * g->max_degree * (opts->k + 2) + (1u << 16);
+            arena_words = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(arena_words, hub),
+                                                        1ull << 30);
+        }
+    }
+    const uint32_t smax = opts->max_members ? opts->max_members : kDefaultSmax;
+    // workers: threads (thread engine) or warps (warp engine)
+    uint64_t threads = opts->threads ? opts->threads : (uint64_t)di.sms * per_sm * block;
+    threads = std::max<uint64_t>(threads, (uint64_t)block);
+    // keep the search arenas within 40% of free device memory (asked only when
+    // the cached workspace is too small)
+    const uint64_t per_worker = 4ull * arena_words + 8ull * smax;
     uint64_t workers = threads / lanes_per_worker;
-    if (workers * per_worker > budget)
-        workers = std::max<uint64_t>(block / lanes_per_worker, budget / per_worker);
+    if (workers * 4ull * arena_words > ws.arena_bytes || workers * 8ull * smax > ws.sbuf_bytes) {
+        size_t free_b = 0, total_b = 0;
+        CK(cudaMemGetInfo(&free_b, &total_b));
+        const uint64_t budget = (uint64_t)((double)(free_b + ws.arena_bytes + ws.sbuf_bytes) * 0.4);
+        if (workers * per_worker > budget)
+            workers = std::max<uint64_t>(block / lanes_per_worker, budget / per_worker);
+    }
     threads = (workers * lanes_per_worker + block - 1) / block * block;
     workers = threads / lanes_per_worker;
 
@@ -532,15 +656,17 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
     }
     uint64_t out_words = 0;
     if (opts->emit) {
-        out_words = opts->out_words ? opts->out_words : (64ull << 20);
-        if ((rc = grow((void**)&ws.d_out, &ws.out_bytes, out_words * 4ull))) return rc;
+        // the warp engine streams through two buffers of out_words each
+        out_words = opts->out_words ? opts->out_words : (warp ? (16ull << 20) : (64ull << 20));
+        if ((rc = grow((void**)&ws.d_out, &ws.out_bytes, out_words * 4ull * (warp ? 2 : 1))))
+            return rc;
     }
     // the warp engine splits unfinished trees (batched / ordered schedules)
     const uint32_t split_min = (!warp || opts->schedule == GMK_SCHEDULE_PLAIN)
                                    ? 0u
                                    : (opts->split_min_nodes ? opts->split_min_nodes : 64u);
     unsigned long long split_word_cap = 0, split_idx_cap = 0;
-    if (split_min) {
+    if (warp) {   // split records: load balance, record-buffer draining, and round bookkeeping
         split_word_cap = std::max<unsigned long long>(1ull << 22, workers * 4096ull);
         split_idx_cap = std::max<unsigned long long>(1ull << 16, workers * 64ull);
         for (int b = 0; b < 2; ++b) {
@@ -558,6 +684,7 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
     Counters h;
     unsigned long long tasks_total = 0, tasks_done = 0;
     uint32_t rounds = 0;
+    int warp_emit_rc = GMK_OK;
     CK(cudaEventRecord(g->ev0, g->stream));
     if (!warp) {
         enumerate_kernel<<<grid, kBlock, 0, g->stream>>>(
@@ -584,11 +711,11 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
         a.sbuf = ws.d_sbuf;
         a.smax = smax;
         a.pair_limit = pair_limit;
-        a.n_tasks = n_tasks;
         a.chunk = chunk;
         a.chunks_per_root = chunks_per_root;
         a.root_order = d_order;
         a.root_base = root_begin;
+        a.n_roots = root_end - root_begin;
         a.split_min_nodes = split_min;
         a.limit = opts->result_limit;
         a.out_buf = opts->emit ? ws.d_out : nullptr;
@@ -602,41 +729,77 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
             CK(cudaMemsetAsync(g->d_root_nodes, 0, 8ull * g->nl, g->stream));
             a.root_nodes = g->d_root_nodes;
         }
-        unsigned long long queue_len = my_tasks;
-        int cur = 0;
+        // Record mode streams: each round writes one of two record buffers,
+        // and while the next round runs the host hands the previous round's
+        // records to the sink.  A round winds down (splits its tasks into the
+        // next round) once its buffer is half full.
+        uint32_t* outb[2] = {ws.d_out, opts->emit ? ws.d_out + out_words : nullptr};
+        a.drain_at = opts->emit ? std::max<uint64_t>(1, out_words / 2) : 0;
+        unsigned long long root_next = 0, n_records = 0;
+        int cur = 0, pending = -1;
+        unsigned long long pending_words = 0;
+        int sink_rc = GMK_OK;
         const auto host_t0 = std::chrono::steady_clock::now();
         for (int round = 0;; ++round) {
-            a.round = round;
-            a.queue_len = queue_len;
-            a.cur_words = round ? ws.d_split_words[cur] : nullptr;
-            a.cur_idx = round ? ws.d_split_idx[cur] : nullptr;
+            a.n_records = n_records;
+            a.root_task_base = root_next;
+            a.queue_len = n_records + (my_tasks - root_next);
+            a.cur_words = ws.d_split_words[cur];
+            a.cur_idx = ws.d_split_idx[cur];
             a.next.words = ws.d_split_words[cur ^ 1];
             a.next.idx = ws.d_split_idx[cur ^ 1];
             a.next.used = &g->d_rc->next_used;
             a.next.count = &g->d_rc->next_count;
+            a.next.count_fail = &g->d_rc->next_fail;
+            a.next.refused = &g->d_rc->split_refused;
             a.next.word_cap = split_word_cap;
             a.next.idx_cap = split_idx_cap;
+            a.out_buf = opts->emit ? outb[round & 1] : nullptr;
             CK(cudaMemsetAsync(g->d_rc, 0, sizeof(RoundCounters), g->stream));
+            CK(cudaMemsetAsync(&g->d_rc->out_fail, 0xFF, 2 * sizeof(unsigned long long), g->stream));
             enumerate_warp_kernel<<<grid, kWBlock, 0, g->stream>>>(a);
             CK(cudaGetLastError());
+            if (pending >= 0 && sink_rc == GMK_OK) {
+                sink_rc = deliver_records(g, outb[pending], pending_words, sink, user);
+                pending = -1;
+            }
             RoundCounters r;
             CK(cudaMemcpyAsync(&r, g->d_rc, sizeof(r), cudaMemcpyDeviceToHost, g->stream));
             CK(cudaMemcpyAsync(&h, g->d_ctr, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
             CK(cudaStreamSynchronize(g->stream));
             ++rounds;
-            tasks_total += queue_len;
-            tasks_done += std::min<unsigned long long>(r.tasks_done, queue_len);
-            if (h.error || h.stop || r.next_count == 0) break;
+            tasks_total += a.queue_len;
+            tasks_done += std::min<unsigned long long>(r.tasks_done, a.queue_len);
+            if (opts->emit) {
+                // records end where the first one found no room
+                pending = round & 1;
+                pending_words = std::min({r.out_pos, (unsigned long long)out_words, r.out_fail});
+            }
+            const unsigned long long consumed = std::min(r.next_task, a.queue_len);
+            if (consumed > n_records) root_next += consumed - n_records;
+            if (h.error == gmk::TASK_E_OUTBUF) {
+                static const char* why[] = {"", "unentered root frame", "nothing pending",
+                                            "split words full", "split index full"};
+                g_cuda_err = std::string("record deferral failed: ") +
+                             why[r.split_refused >= 0 && r.split_refused <= 4 ? r.split_refused : 0];
+            }
+            if (h.error || h.stop || sink_rc != GMK_OK) break;
+            if (std::min({r.next_count, split_idx_cap, r.next_fail}) == 0 && root_next >= my_tasks)
+                break;
             if (watchdog_ns) {
                 const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() -
                                                                 host_t0).count();
                 if (el * 1e9 > (double)watchdog_ns) { h.error = gmk::TASK_E_TIMEOUT; break; }
             }
-            queue_len = r.next_count;
+            n_records = std::min({r.next_count, split_idx_cap, r.next_fail});
             cur ^= 1;
         }
         CK(cudaEventRecord(g->ev1, g->stream));
         CK(cudaStreamSynchronize(g->stream));
+        if (pending >= 0 && sink_rc == GMK_OK && !h.error)
+            sink_rc = deliver_records(g, outb[pending], pending_words, sink, user);
+        if (sink_rc < 0 && sink_rc != GMK_E_SINK) return sink_rc;
+        if (sink_rc == GMK_E_SINK) warp_emit_rc = GMK_E_SINK;
         if (opts->root_nodes) {
             std::vector<unsigned long long> rn(g->nl);
             CK(cudaMemcpy(rn.data(), g->d_root_nodes, 8ull * g->nl, cudaMemcpyDeviceToHost));
@@ -662,8 +825,10 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
         case gmk::TASK_E_ARENA: return GMK_E_ARENA;
         case gmk::TASK_E_SMAX: return GMK_E_SMAX;
         case gmk::TASK_E_TIMEOUT: return GMK_E_TIMEOUT;
+        case gmk::TASK_E_OUTBUF: return GMK_E_OUTBUF;
         default: return GMK_E_CUDA;
     }
+    if (warp) return warp_emit_rc;
     if (opts->emit) {
         if (h.out_pos > out_words) return GMK_E_OUTBUF;
         std::vector<uint32_t> rec(h.out_pos);

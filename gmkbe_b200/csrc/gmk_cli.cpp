@@ -99,15 +99,10 @@ int main(int argc, char** argv) {
     Printer p;
     o.emit = quiet ? 1 : 0;
     gmk_stats st;
-    for (;;) {
-        rc = checkpoint.empty()
-                 ? gmk_enumerate(g, &o, quiet ? print_result : nullptr, &p, &st)
-                 : gmk_enumerate_resumable(g, &o, checkpoint.c_str(), batch_roots, 0,
-                                           quiet ? print_result : nullptr, &p, &st);
-        if (rc != GMK_E_OUTBUF) break;
-        o.out_words = (o.out_words ? o.out_words : (64ull << 20)) * 4;   // retry, bigger buffer
-        p.n = 0;
-    }
+    // results stream through the library's record buffers; no retry is needed
+    rc = checkpoint.empty() ? gmk_enumerate(g, &o, quiet ? print_result : nullptr, &p, &st)
+                            : gmk_enumerate_resumable(g, &o, checkpoint.c_str(), batch_roots, 0,
+                                                      quiet ? print_result : nullptr, &p, &st);
     if (rc) {
         std::fprintf(stderr, "gmk: %s (%s)\n", gmk_strerror(rc), gmk_last_cuda_error());
         gmk_graph_free(g);

@@ -55,6 +55,10 @@ int gmk_graph_from_csr(const uint32_t* offsets, const uint32_t* adj, uint32_t n,
 /* Sizes of a loaded graph (any pointer may be NULL). */
 int gmk_graph_info(const gmk_graph* g, uint32_t* n, uint32_t* n_left, uint64_t* adj_len);
 
+/* 64-bit order-dependent hash of the graph's CSR, computed on the device at
+ * load; the identity that checkpoints and tuning caches record. */
+int gmk_graph_fingerprint(const gmk_graph* g, uint64_t* out);
+
 /* Releases device memory (the CSR and any cached enumeration workspace). */
 void gmk_graph_free(gmk_graph* g);
 

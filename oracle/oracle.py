@@ -27,6 +27,11 @@ def bppivot_path() -> str:
     return os.path.join(HERE, "_ref", "bppivot")
 
 
+def refgpu_path() -> str:
+    """The reference's own GPU enumerator (make -C oracle refgpu)."""
+    return os.path.join(HERE, "_ref", "gmkbpe")
+
+
 # ----------------------------------------------------------------------------- hashing
 
 def _mix64(z: int) -> int:
@@ -217,6 +222,51 @@ def run_bppivot(graph_path: str, k: int, result_limit: int = 0, output: bool = F
     return {"count": int(cnt.group(1)) if cnt else None,
             "branch_ms": int(br.group(1)) if br else None,
             "wall_s": wall, "text": text if output else None}
+
+
+# ----------------------------------------------------------------------------- reference GPU binary
+
+_RESULT = re.compile(r"^Result \d+: X: ([0-9 ]*)\| Y: ([0-9 ]*)$")
+_RUNTIME = re.compile(r"Running Time:\s*([0-9.eE+-]+)\s*ms")
+
+
+def parse_reference_results(text: str, n_left: int):
+    """The reference's `Result N: X: x.. | Y: y..` lines (src/output.cuh) as
+    sorted (X, Y) tuples of global ids (Y ids below n_left are shifted)."""
+    for line in text.splitlines():
+        m = _RESULT.match(line.rstrip("\n"))
+        if not m:
+            continue
+        x = tuple(sorted(int(t) for t in m.group(1).split()))
+        y = [int(t) for t in m.group(2).split()]
+        y = tuple(sorted(v if v >= n_left else v + n_left for v in y))
+        yield x, y
+
+
+def run_reference_gpu(graph_path: str, k: int, result_limit: int = 10_000_000,
+                      output: bool = False, device: int = 0, timeout: float | None = None) -> dict:
+    """Runs `gmkbpe -f <graph> -k k -r limit -q 0|1 -d device` on a private
+    copy of the graph's directory (its time recorder writes a JSON next to the
+    input).  Returns running_ms, the printed result lines' text (output=True)
+    and the exit status."""
+    exe = refgpu_path()
+    tmpdir = tempfile.mkdtemp(prefix="gmkbpe_")
+    link = os.path.join(tmpdir, "g.graph.bin")
+    os.symlink(os.path.abspath(graph_path), link)
+    cmd = [exe, "-f", link, "-k", str(k), "-r", str(result_limit), "-q", "1" if output else "0",
+           "-d", str(device)]
+    import shutil
+    import time
+    t0 = time.perf_counter()
+    with tempfile.TemporaryFile() as f:
+        p = subprocess.run(cmd, stdout=f, stderr=subprocess.STDOUT, timeout=timeout)
+        wall = time.perf_counter() - t0
+        f.seek(0)
+        text = f.read().decode(errors="replace")
+    shutil.rmtree(tmpdir, ignore_errors=True)
+    m = _RUNTIME.search(text)
+    return {"returncode": p.returncode, "running_ms": float(m.group(1)) if m else None,
+            "wall_s": wall, "text": text}
 
 
 # ----------------------------------------------------------------------------- brute force

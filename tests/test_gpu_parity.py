@@ -83,9 +83,32 @@ def test_ordered_schedule_same_set(golden, graphs):
 def test_thread_and_arena_shapes_do_not_change_the_set(golden, graphs):
     case = next(c for c in golden["cases"] if c["graph"] == "er200" and c["k"] == 1)
     # 4096 threads = 128 warps: few enough that warps take many tasks each
-    for threads, pair_limit in [(4096, 1), (8192, 64), (0, 1 << 20)]:
+    for threads, pair_limit in [(4096, 64), (8192, 256), (0, 1 << 20)]:
         st = graphs("er200").enumerate(k=1, threads=threads, pair_limit=pair_limit)
         assert st.summary() == _summary(case), (threads, pair_limit)
+    # pair_limit 1 turns the node rules off almost everywhere: a far larger tree
+    small = next(c for c in golden["cases"] if c["graph"] == "er60" and c["k"] == 1)
+    assert graphs("er60").enumerate(k=1, pair_limit=1).summary() == _summary(small)
+
+
+@pytest.mark.parametrize("out_words", [600, 4096])
+def test_streamed_records_through_small_buffers(golden, graphs, out_words):
+    # a record buffer far smaller than the output: rounds wind down whenever
+    # it is half full, and the host drains it while the next round runs
+    case = next(c for c in golden["cases"] if c["graph"] == "er60" and c["k"] == 2)
+    got = []
+    st = graphs("er60").enumerate(k=2, sink=lambda x, y: got.append((x, y)) and False,
+                                  out_words=out_words)
+    assert st.rounds > 5
+    assert O.set_summary(got) == _summary(case) == st.summary()
+    assert len(got) == len(set(got))
+
+
+def test_streamed_records_with_limit(graphs):
+    got = []
+    st = graphs("er200").enumerate(k=1, result_limit=30_000, out_words=2048,
+                                   sink=lambda x, y: got.append((x, y)) and False)
+    assert st.count == 30_000 == len(got) == len(set(got))
 
 
 def test_emitted_sets_equal_reference_sets(graphs):
@@ -206,3 +229,17 @@ def test_limited_run_at_full_size():
     assert len(set(sample.results)) == 2000
     for x, y in sample.results[::100]:
         assert O.classify(g, 1, x, y) == 2
+
+
+def test_autotuner_picks_a_setting_and_caches_it(tmp_path):
+    from gmkbe_b200 import autotune
+    cache = str(tmp_path / "tune.json")
+    with G.Graph.load(golden_graph_path("er200")) as g:
+        first = autotune.tune(g, 1, result_limit=20_000, repeats=1, cache_path=cache)
+        assert not first["cached"] and first["results"] == 20_000
+        assert first["settings"] in [t["settings"] for t in first["trials"]]
+        again = autotune.tune(g, 1, result_limit=20_000, cache_path=cache)
+        assert again["cached"] and again["settings"] == first["settings"]
+        # the tuned settings keep the set
+        case_full = g.enumerate(k=1).summary()
+        assert g.enumerate(k=1, **first["settings"]).summary() == case_full

@@ -49,9 +49,10 @@ def _peaks():
     return 6650.0, "fallback"
 
 
-def _traffic_per_launch():
-    """DRAM bytes per enumerate_kernel launch from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "enumerate_kernel_cl20k.json")
+def _traffic_per_launch(kernel: str):
+    """DRAM bytes (read + write) per launch of `kernel` on this workload, from
+    the committed ncu summary (profiles/<kernel>_cl20k.json), or None."""
+    p = os.path.join(ROOT, "profiles", f"{kernel}_cl20k.json")
     if os.path.exists(p):
         with open(p) as f:
             return json.load(f).get("dram_bytes_per_launch")
@@ -247,7 +248,9 @@ def run_gmk(args, world, rank, local):
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": _traffic_per_launch(),
+                         "frac": achieved / peak,
+                         "traffic": _traffic_per_launch("enumerate_warp_kernel" if args.engine == "warp"
+                                                        else "enumerate_kernel"),
                          "peak_source": peak_kind,
                          "kernel": ("enumerate_warp_kernel" if args.engine == "warp"
                                     else "enumerate_kernel"),

@@ -5,7 +5,8 @@ input, same -f/-k/-r/-d command line (gmkbe_b200/gmk, `python -m gmkbe_b200`),
 and a C ABI (include/gmk.h, libgmk.so) for embedding.  The search runs only
 on the GPU; without the built library every entry point raises.
 """
-from .api import (EXPORTS, LIB_PATH, Graph, GmkError, Stats, load_library,  # noqa: F401
-                  result_hash)
+from .api import (EXPORTS, LIB_PATH, Graph, GmkError, Stats, enumerate_batch,  # noqa: F401
+                  load_library, result_hash)
 
-__all__ = ["Graph", "GmkError", "Stats", "load_library", "result_hash", "EXPORTS", "LIB_PATH"]
+__all__ = ["Graph", "GmkError", "Stats", "enumerate_batch", "load_library", "result_hash",
+           "EXPORTS", "LIB_PATH"]

@@ -24,7 +24,7 @@ LIB_PATH = os.environ.get("GMK_LIBRARY") or os.path.join(_PKG, "libgmk.so")
 # entry points declared in include/gmk.h
 EXPORTS = ("gmk_graph_load", "gmk_graph_from_csr", "gmk_graph_info", "gmk_graph_fingerprint",
            "gmk_graph_free",
-           "gmk_opts_default", "gmk_enumerate", "gmk_enumerate_resumable",
+           "gmk_opts_default", "gmk_enumerate", "gmk_enumerate_batch", "gmk_enumerate_resumable",
            "gmk_enumerate_noalloc", "gmk_result_hash", "gmk_strerror", "gmk_last_cuda_error",
            "gmk_abi_version", "gmk_root_features", "gmk_mlp_create", "gmk_mlp_free",
            "gmk_mlp_params", "gmk_mlp_gradient", "gmk_mlp_train", "gmk_mlp_predict")
@@ -92,6 +92,9 @@ def load_library(path: str = LIB_PATH):
     lib.gmk_opts_default.restype = None
     lib.gmk_enumerate.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Opts), SINK, ctypes.c_void_p,
                                   ctypes.POINTER(_Stats)]
+    lib.gmk_enumerate_batch.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_uint32, P32,
+                                        ctypes.POINTER(ctypes.POINTER(ctypes.c_float)),
+                                        ctypes.POINTER(_Opts), ctypes.POINTER(_Stats)]
     lib.gmk_enumerate_resumable.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Opts), ctypes.c_char_p,
                                             ctypes.c_uint32, ctypes.c_uint32, SINK,
                                             ctypes.c_void_p, ctypes.POINTER(_Stats)]
@@ -141,6 +144,33 @@ class Stats:
 
     def summary(self) -> tuple[int, int, int]:
         return self.count, self.hash_sum, self.hash_xor
+
+
+def enumerate_batch(graphs, ks, schedule: str = "batched", task_costs=None, **tuning) -> list:
+    """gmk_enumerate_batch: full enumeration of several graphs (all on one
+    device) in one run of launches; ks[i] is graph i's k.  Returns one Stats
+    per graph."""
+    lib = load_library()
+    n = len(graphs)
+    o, _ = graphs[0]._opts(int(ks[0]), 0, schedule, tuning.get("chunk", 0), tuning.get("threads", 0),
+                           tuning.get("arena_words", 0), tuning.get("max_members", 0),
+                           tuning.get("watchdog_ms", 0), tuning.get("pair_limit", 0), None, 0, 1,
+                           "warp", tuning.get("split_min_nodes", 0), 0, 0)
+    hs = (ctypes.c_void_p * n)(*[g._h.value for g in graphs])
+    karr = np.ascontiguousarray(ks, dtype=np.uint32)
+    PF = ctypes.POINTER(ctypes.c_float)
+    costs_keep = []
+    costs = None
+    if task_costs is not None:
+        costs = (PF * n)()
+        for i, c in enumerate(task_costs):
+            c = np.ascontiguousarray(c, dtype=np.float32)
+            costs_keep.append(c)
+            costs[i] = c.ctypes.data_as(PF)
+    outs = (_Stats * n)()
+    _check(lib.gmk_enumerate_batch(hs, n, karr.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                                   costs, ctypes.byref(o), outs))
+    return [Graph._stats(outs[i], None) for i in range(n)]
 
 
 def result_hash(x, y) -> tuple[int, int]:

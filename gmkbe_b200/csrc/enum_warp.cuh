@@ -120,8 +120,9 @@ __device__ __forceinline__ unsigned long long warp_sum64(unsigned long long v) {
 template <class T>
 __device__ __forceinline__ T bcast(T v) { return __shfl_sync(kFull, v, 0); }
 
-// Next-round task list: records [ns, cnt0, cnt1, sid[ns], smc[ns],
+// Next-round task list: records [ns, cnt0, cnt1, graph, sid[ns], smc[ns],
 // frame[F_WORDS], list0[2 cnt0], list1[2 cnt1]] addressed by an index array.
+constexpr uint32_t kRecHeader = 4;
 struct SplitBuf {
     uint32_t* words;
     unsigned long long* idx;
@@ -148,6 +149,7 @@ struct Ctx {
     GraphView g;
     EdgeHash eh;
     uint32_t k;
+    uint32_t gid;                                // graph of the current task (batched launches)
     uint32_t* arena;
     uint32_t cap;
     uint32_t* sid;
@@ -931,30 +933,15 @@ __device__ __forceinline__ uint32_t frame_list_words(const uint32_t* f) {
     return 2 * (c0 + c1);
 }
 
-// Writes every pending frame on the path from `cur` to the root as a task of
-// the next round.  All-or-nothing: returns false (and writes nothing) when
-// the buffer cannot take them all.
-__device__ bool split_path(Ctx& t, const SplitBuf& sb, uint32_t cur) {
-    // sizes first
-    unsigned long long words = 0, recs = 0;
-    for (uint32_t x = cur; x != kNoPos; x = t.arena[x + F_PARENT_SLOT]) {
-        const uint32_t* f = t.arena + x;
-        if (!frame_pending(f, x == cur)) continue;
-        if ((f[F_FLAGS] & FL_ROOT) && !(f[F_FLAGS] & FL_ENTERED)) {
-            if (t.lane == 0) atomicCAS(sb.refused, 0, 1);
-            return false;
-        }
-        words += 3ull + 2ull * f[F_NS] + F_WORDS + frame_list_words(f);
-        ++recs;
-    }
-    if (recs == 0) {
-        if (t.lane == 0) atomicCAS(sb.refused, 0, 2);
-        return false;
-    }
-    // Reservations are plain atomic adds (thousands of warps split at once
-    // when a round winds down).  Positions only grow, so once one reservation
-    // fails every later one fails too: the records below count_fail are the
-    // complete, written ones.  A failed word reservation is simply unused.
+// Reserves `words` words and `recs` index slots of the next round's task list
+// (warp-uniform result).  Reservations are plain atomic adds: thousands of
+// warps split at once when a round winds down.  Positions only grow, so once
+// one reservation fails every later one fails too: the records below
+// count_fail are the complete, written ones.  A failed word reservation is
+// simply left unused.
+__device__ bool reserve_records(Ctx& t, const SplitBuf& sb, unsigned long long words,
+                                unsigned long long recs, unsigned long long* w0_out,
+                                unsigned long long* r0_out) {
     unsigned long long w0 = 0, r0 = 0;
     int ok = 0;
     if (t.lane == 0) {
@@ -968,8 +955,48 @@ __device__ bool split_path(Ctx& t, const SplitBuf& sb, uint32_t cur) {
         }
     }
     if (!bcast(ok)) return false;
-    w0 = bcast(w0);
-    r0 = bcast(r0);
+    *w0_out = bcast(w0);
+    *r0_out = bcast(r0);
+    return true;
+}
+
+// Copies a record of this round unchanged into the next round's task list
+// (a round that winds down hands its queued records on instead of starting
+// them).  False when the list has no room.
+__device__ bool forward_record(Ctx& t, const SplitBuf& sb, const uint32_t* r) {
+    const uint32_t ns = r[0], c0 = r[1], c1 = r[2];
+    const unsigned long long words = kRecHeader + 2ull * ns + F_WORDS + 2ull * (c0 + c1);
+    unsigned long long w0 = 0, r0 = 0;
+    if (!reserve_records(t, sb, words, 1, &w0, &r0)) return false;
+    uint32_t* dst = sb.words + w0;
+    for (unsigned long long i = t.lane; i < words; i += 32) dst[i] = r[i];
+    if (t.lane == 0) sb.idx[r0] = w0;
+    __syncwarp();
+    return true;
+}
+
+// Writes every pending frame on the path from `cur` to the root as a task of
+// the next round.  All-or-nothing: returns false (and writes nothing) when
+// the buffer cannot take them all.
+__device__ bool split_path(Ctx& t, const SplitBuf& sb, uint32_t cur) {
+    // sizes first
+    unsigned long long words = 0, recs = 0;
+    for (uint32_t x = cur; x != kNoPos; x = t.arena[x + F_PARENT_SLOT]) {
+        const uint32_t* f = t.arena + x;
+        if (!frame_pending(f, x == cur)) continue;
+        if ((f[F_FLAGS] & FL_ROOT) && !(f[F_FLAGS] & FL_ENTERED)) {
+            if (t.lane == 0) atomicCAS(sb.refused, 0, 1);
+            return false;
+        }
+        words += kRecHeader + 2ull * f[F_NS] + F_WORDS + frame_list_words(f);
+        ++recs;
+    }
+    if (recs == 0) {
+        if (t.lane == 0) atomicCAS(sb.refused, 0, 2);
+        return false;
+    }
+    unsigned long long w0 = 0, r0 = 0;
+    if (!reserve_records(t, sb, words, recs, &w0, &r0)) return false;
     unsigned long long wp = w0, rp = r0;
     for (uint32_t x = cur; x != kNoPos; x = t.arena[x + F_PARENT_SLOT]) {
         const uint32_t* f = t.arena + x;
@@ -979,16 +1006,17 @@ __device__ bool split_path(Ctx& t, const SplitBuf& sb, uint32_t cur) {
         const uint32_t c0 = (f[F_FLAGS] & FL_G0) ? 0u : f[F_CNT0];
         const uint32_t c1 = (f[F_FLAGS] & FL_G1) ? 0u : f[F_CNT1];
         uint32_t* r = sb.words + wp;
-        if (t.lane == 0) { r[0] = ns; r[1] = c0; r[2] = c1; sb.idx[rp] = wp; }
-        for (uint32_t i = t.lane; i < ns; i += 32) { r[3 + i] = t.sid[i]; r[3 + ns + i] = t.smc[i]; }
-        uint32_t* fr = r + 3 + 2 * ns;
+        if (t.lane == 0) { r[0] = ns; r[1] = c0; r[2] = c1; r[3] = t.gid; sb.idx[rp] = wp; }
+        uint32_t* rs = r + kRecHeader;
+        for (uint32_t i = t.lane; i < ns; i += 32) { rs[i] = t.sid[i]; rs[ns + i] = t.smc[i]; }
+        uint32_t* fr = rs + 2 * ns;
         if (t.lane < F_WORDS) fr[t.lane] = f[t.lane];
         uint32_t* lr = fr + F_WORDS;
         const uint32_t* a0 = t.arena + f[F_OFF0];
         const uint32_t* a1 = t.arena + f[F_OFF1];
         for (uint32_t i = t.lane; i < 2 * c0; i += 32) lr[i] = a0[i];
         for (uint32_t i = t.lane; i < 2 * c1; i += 32) lr[2 * c0 + i] = a1[i];
-        wp += 3ull + 2ull * ns + F_WORDS + 2ull * (c0 + c1);
+        wp += kRecHeader + 2ull * ns + F_WORDS + 2ull * (c0 + c1);
         ++rp;
     }
     __syncwarp();
@@ -1106,19 +1134,20 @@ __device__ unsigned long long run_record(Ctx& t, const Outputs& o, const uint32_
     if (ns > t.smax) { fail(t, o, TASK_E_SMAX); return 0; }
     if (F_WORDS + 2ull * (c0 + c1) > t.cap) { fail(t, o, TASK_E_ARENA); return 0; }
     uint32_t nv = 0;
+    const uint32_t* rs = r + kRecHeader;
     for (uint32_t base = 0; base < ns; base += 32) {
         const uint32_t i = base + t.lane;
         bool isv = false;
         if (i < ns) {
-            const uint32_t v = r[3 + i];
+            const uint32_t v = rs[i];
             t.sid[i] = v;
-            t.smc[i] = r[3 + ns + i];
+            t.smc[i] = rs[ns + i];
             isv = side_of(t.g, v) != 0;
         }
         nv += __popc(__ballot_sync(kFull, isv));
     }
     t.ns = ns; t.nss.b = nv; t.nss.a = ns - nv;
-    const uint32_t* fr = r + 3 + 2 * ns;
+    const uint32_t* fr = rs + 2 * ns;
     Hdr h = read_hdr(fr);
     h.off.a = F_WORDS;
     h.off.b = F_WORDS + 2 * c0;

@@ -112,11 +112,26 @@ constexpr int kWarpsPerBlock = kWBlock / 32;
 #endif
 constexpr uint32_t kDefaultWarpArena = 1u << 18;
 
-struct WarpArgs {
+// One graph of a launch.  A launch enumerates one graph (gmk_enumerate) or a
+// batch of graphs (gmk_enumerate_batch); each has its own k, chunking, root
+// order and counters, and its root tasks occupy [task_begin, task_begin +
+// n_roots * chunks) of the launch's task numbering.
+struct GraphTask {
     gmk::GraphView g;
     gmk::warp::EdgeHash eh;
     uint32_t k;
-    Counters* ctr;
+    uint32_t chunk, n_roots, root_base;
+    const uint32_t* root_order;
+    Counters* ctr;                     // counts, hashes, nodes, work of this graph
+    unsigned long long* root_nodes;    // optional per-root node log
+    unsigned long long task_begin;
+};
+
+struct WarpArgs {
+    GraphTask single;                  // the graph of a one-graph launch (kernel parameter)
+    const GraphTask* graphs;           // the graphs of a batch launch
+    uint32_t n_graphs;
+    Counters* ctr;                     // stop / error / watchdog origin of the launch
     RoundCounters* rc;
     uint32_t* arenas;
     uint32_t arena_words;
@@ -129,10 +144,6 @@ struct WarpArgs {
     unsigned long long root_task_base;
     unsigned long long queue_len;
     unsigned long long drain_at;       // record mode: wind the round down past this out_pos
-    uint32_t chunk, chunks_per_root;
-    const uint32_t* root_order;
-    uint32_t root_base;                // first root position of this call
-    uint32_t n_roots;                  // roots in this call
     const uint32_t* cur_words;         // split records of the previous round
     const unsigned long long* cur_idx;
     gmk::warp::SplitBuf next;
@@ -142,9 +153,25 @@ struct WarpArgs {
     unsigned long long out_cap;
     unsigned long long watchdog_ns;
     uint32_t shard, nshards;
-    unsigned long long* root_nodes;    // optional per-root node log
 };
 
+// Points the warp's context and counters at graph gid of the launch.  A
+// one-graph launch reads its graph from the kernel parameters, so the values
+// stay rematerialisable instead of occupying registers.
+template <bool kBatch>
+__device__ __forceinline__ const GraphTask& use_graph(const WarpArgs& a, uint32_t gid,
+                                                     gmk::warp::Ctx& t, gmk::Outputs& o) {
+    const GraphTask& G = kBatch ? a.graphs[gid] : a.single;
+    t.g = G.g;
+    t.eh = G.eh;
+    t.k = G.k;
+    t.gid = gid;
+    o.count = &G.ctr->count; o.hash_sum = &G.ctr->hash_sum; o.hash_xor = &G.ctr->hash_xor;
+    o.nodes = &G.ctr->nodes; o.work = &G.ctr->work;
+    return G;
+}
+
+template <bool kBatch>
 __global__ void __launch_bounds__(kWBlock, GMK_WARP_MIN_BLOCKS) enumerate_warp_kernel(const WarpArgs a) {
     __shared__ uint32_t s_sat[kWarpsPerBlock][gmk::kSatCap];
     __shared__ uint32_t s_src[kWarpsPerBlock][gmk::warp::kSrcCap];
@@ -170,7 +197,7 @@ __global__ void __launch_bounds__(kWBlock, GMK_WARP_MIN_BLOCKS) enumerate_warp_k
         o.deadline_ns = bcast(t0) + a.watchdog_ns;
     }
     Ctx t;
-    t.g = a.g; t.eh = a.eh; t.k = a.k;
+    use_graph<kBatch>(a, 0, t, o);
     t.arena = a.arenas + wid * a.arena_words; t.cap = a.arena_words;
     t.sid = a.sbuf + wid * 2ull * a.smax; t.smc = t.sid + a.smax; t.smax = a.smax;
     t.ns = 0; t.nss.a = t.nss.b = 0;
@@ -213,21 +240,37 @@ __global__ void __launch_bounds__(kWBlock, GMK_WARP_MIN_BLOCKS) enumerate_warp_k
         if (stop || j >= a.queue_len) break;
         if (lane == 0) atomicAdd(&a.rc->tasks_done, 1ull);
         if (j >= a.n_records) {
+            const unsigned long long id = (a.root_task_base + (j - a.n_records)) * a.nshards + a.shard;
+            // the graph whose task range holds id (the last with task_begin <= id)
+            uint32_t lo = 0;
+            if (kBatch) {
+                uint32_t hi = a.n_graphs;
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (a.graphs[mid].task_begin <= id) lo = mid; else hi = mid;
+                }
+            }
+            const GraphTask& G = use_graph<kBatch>(a, lo, t, o);
             // chunk-major: every root's first chunk of children, then every
             // root's second, ... (the low-degree V children come first)
-            const unsigned long long id = (a.root_task_base + (j - a.n_records)) * a.nshards + a.shard;
-            const uint32_t r = a.root_base + (uint32_t)(id % a.n_roots);
-            const uint32_t c = (uint32_t)(id / a.n_roots);
-            const uint32_t root = a.root_order ? a.root_order[r] : r;
-            const uint32_t first = a.g.nl + c * a.chunk;
-            const unsigned long long end = (unsigned long long)first + a.chunk;
-            const uint32_t last = end < a.g.n ? (uint32_t)end : a.g.n;
+            const unsigned long long local = id - G.task_begin;
+            const uint32_t r = G.root_base + (uint32_t)(local % G.n_roots);
+            const uint32_t c = (uint32_t)(local / G.n_roots);
+            const uint32_t root = G.root_order ? G.root_order[r] : r;
+            const uint32_t first = t.g.nl + c * G.chunk;
+            const unsigned long long end = (unsigned long long)first + G.chunk;
+            const uint32_t last = end < t.g.n ? (uint32_t)end : t.g.n;
             const unsigned long long nodes = run_root(t, o, root, first, last, sb, lim);
-            if (a.root_nodes && lane == 0) atomicAdd(a.root_nodes + root, nodes);
+            if (G.root_nodes && lane == 0) atomicAdd(G.root_nodes + root, nodes);
         } else {
             const uint32_t* rec = a.cur_words + a.cur_idx[j];
-            const unsigned long long nodes = run_record(t, o, rec, sb, lim);
-            if (a.root_nodes && lane == 0) atomicAdd(a.root_nodes + rec[3], nodes);
+            const GraphTask& G = use_graph<kBatch>(a, kBatch ? rec[3] : 0u, t, o);
+            // a round that winds down hands its queued records on unchanged
+            if (!(sb && draining(lim) && forward_record(t, *sb, rec))) {
+                const unsigned long long nodes = run_record(t, o, rec, sb, lim);
+                if (G.root_nodes && lane == 0)
+                    atomicAdd(G.root_nodes + rec[gmk::warp::kRecHeader], nodes);
+            }
         }
         flush(t, o);
         if (t.err) break;
@@ -310,6 +353,8 @@ struct Workspace {
     size_t sbuf_bytes = 0;
     uint32_t* d_out = nullptr;
     size_t out_bytes = 0;
+    void* d_graphs = nullptr;     // the launch's GraphTask array
+    size_t graphs_bytes = 0;
     // two split buffers (this round's records, the next round's)
     uint32_t* d_split_words[2] = {nullptr, nullptr};
     size_t split_words_bytes[2] = {0, 0};
@@ -557,32 +602,36 @@ void gmk_opts_default(gmk_opts* o) {
     o->schedule = GMK_SCHEDULE_BATCHED;
 }
 
-int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user, gmk_stats* out) {
-    if (!g || !opts || !out) return GMK_E_INVAL;
-    if (opts->k < 1 || opts->k > 15) return GMK_E_INVAL;
-    if (opts->emit && !sink) return GMK_E_INVAL;
-    if (opts->schedule < GMK_SCHEDULE_PLAIN || opts->schedule > GMK_SCHEDULE_ORDERED)
-        return GMK_E_INVAL;
-    if (opts->schedule == GMK_SCHEDULE_ORDERED && !opts->task_cost) return GMK_E_INVAL;
-    if (opts->nshards && opts->shard >= opts->nshards) return GMK_E_INVAL;
-    if (opts->engine != GMK_ENGINE_WARP && opts->engine != GMK_ENGINE_THREAD) return GMK_E_INVAL;
-    if (opts->root_nodes && opts->engine != GMK_ENGINE_WARP) return GMK_E_INVAL;
-    const uint32_t root_end = opts->root_end ? opts->root_end : g->nl;
-    if (root_end > g->nl || opts->root_begin > root_end) return GMK_E_INVAL;
-    const uint32_t root_begin = opts->root_begin;
-    std::memset(out, 0, sizeof(*out));
-    CK(cudaSetDevice(g->device));
-    if (g->nl == 0 || g->n == g->nl || root_begin == root_end) return GMK_OK;   // nothing to do
+}  // extern "C"
 
+namespace {
+
+// One graph of a launch, host side.
+struct GraphJob {
+    gmk_graph* g;
+    uint32_t k;
+    uint32_t root_begin, root_end;
+    const float* task_cost;       // ORDERED schedule: one cost per root
+    uint64_t* root_nodes;         // optional host log
+};
+
+// Enumerates the jobs' graphs (all on one device) in one run of launches and
+// fills outs[i] per graph.  The single-graph call and the batch call share it;
+// a batch needs the warp engine, no records and no sharding (checked by the
+// caller).
+int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, void* user,
+             gmk_stats* outs) {
+    gmk_graph* g0 = jobs[0].g;
+    const int device = g0->device;
     const bool warp = opts->engine == GMK_ENGINE_WARP;
-    Workspace& ws = g_ws[g->device];
+    Workspace& ws = g_ws[device];
     std::lock_guard<std::mutex> lock(ws.mu);
-    DeviceInfo& di = g_dev[g->device];
+    DeviceInfo& di = g_dev[device];
     if (!di.ready) {
         int sms = 0;
-        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device));
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&di.per_sm_warp, enumerate_warp_kernel,
-                                                         kWBlock, 0));
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&di.per_sm_warp,
+                                                         enumerate_warp_kernel<false>, kWBlock, 0));
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&di.per_sm_thread, enumerate_kernel,
                                                          kBlock, 0));
         di.sms = sms;
@@ -591,6 +640,11 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
     const int per_sm = std::max(warp ? di.per_sm_warp : di.per_sm_thread, 1);
     const int block = warp ? kWBlock : kBlock;
     const uint32_t lanes_per_worker = warp ? 32u : 1u;
+    uint32_t max_degree = 0, max_k = 1;
+    for (const GraphJob& j : jobs) {
+        max_degree = std::max(max_degree, j.g->max_degree);
+        max_k = std::max(max_k, j.k);
+    }
     // A warp's arena holds its stack of child lists: a list gathered from a hub's
     // row is up to 2 deg words, and nested lists shrink; (k + 2) such lists
     // per warp cover the depths seen on power-law graphs.
@@ -598,7 +652,7 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
     if (!arena_words) {
         arena_words = warp ? kDefaultWarpArena : kDefaultArena;
         if (warp) {
-            const uint64_t hub = 2ull * g->max_degree * (opts->k + 2) + (1u << 16);
+            const uint64_t hub = 2ull * max_degree * (max_k + 2) + (1u << 16);
             arena_words = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(arena_words, hub),
                                                         1ull << 30);
         }
@@ -620,44 +674,79 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
     }
     threads = (workers * lanes_per_worker + block - 1) / block * block;
     workers = threads / lanes_per_worker;
-
-    // tasks: root x, chunk of first-level children
-    const uint32_t nv = g->n - g->nl;
-    uint32_t chunk = nv;
-    if (opts->schedule != GMK_SCHEDULE_PLAIN) {
-        if (opts->chunk) {
-            chunk = std::min(opts->chunk, nv);
-        } else {
-            // about 8 tasks per worker, but no chunk below 16 children
-            const uint64_t want = 8ull * workers;
-            const uint64_t per_root = (want + g->nl - 1) / g->nl;
-            chunk = (uint32_t)std::max<uint64_t>(16, (nv + per_root - 1) / std::max<uint64_t>(1, per_root));
-            chunk = std::min(chunk, nv);
-        }
-    }
-    const uint32_t chunks_per_root = (nv + chunk - 1) / chunk;
-    const unsigned long long n_tasks = (unsigned long long)(root_end - root_begin) * chunks_per_root;
-    const uint32_t nsh = opts->nshards ? opts->nshards : 1u, sh = opts->nshards ? opts->shard : 0u;
-    const unsigned long long my_tasks = n_tasks > sh ? (n_tasks - sh + nsh - 1) / nsh : 0;
-
     int rc;
     if ((rc = grow((void**)&ws.d_arena, &ws.arena_bytes, workers * 4ull * arena_words))) return rc;
     if ((rc = grow((void**)&ws.d_sbuf, &ws.sbuf_bytes, workers * 8ull * smax))) return rc;
-    const uint32_t* d_order = nullptr;
-    if (opts->schedule == GMK_SCHEDULE_ORDERED) {
-        std::vector<uint32_t> order(g->nl);
-        std::iota(order.begin(), order.end(), 0u);
-        const float* cost = opts->task_cost;
-        std::stable_sort(order.begin(), order.end(),
-                         [cost](uint32_t a, uint32_t b) { return cost[a] > cost[b]; });
-        if ((rc = grow((void**)&g->d_order, &g->order_bytes, 4ull * g->nl))) return rc;
-        CK(cudaMemcpyAsync(g->d_order, order.data(), 4ull * g->nl, cudaMemcpyHostToDevice, g->stream));
-        d_order = g->d_order;
+
+    // per graph: root x with chunks of its first-level children
+    const size_t ng = jobs.size();
+    std::vector<GraphTask> gt(ng);
+    std::vector<uint32_t> chunks(ng), cprs(ng);
+    unsigned long long n_tasks = 0;
+    for (size_t i = 0; i < ng; ++i) {
+        const GraphJob& j = jobs[i];
+        gmk_graph* g = j.g;
+        const uint32_t nv = g->n - g->nl;
+        const uint32_t nroots = j.root_end - j.root_begin;
+        uint32_t chunk = std::max<uint32_t>(nv, 1);
+        if (opts->schedule != GMK_SCHEDULE_PLAIN && nv) {
+            if (opts->chunk) {
+                chunk = std::min(opts->chunk, nv);
+            } else {
+                // about 8 tasks per worker, but no chunk below 16 children
+                const uint64_t want = 8ull * workers;
+                const uint64_t per_root = (want + g->nl - 1) / std::max<uint32_t>(g->nl, 1);
+                chunk = (uint32_t)std::max<uint64_t>(16, (nv + per_root - 1) / std::max<uint64_t>(1, per_root));
+                chunk = std::min(chunk, nv);
+            }
+        }
+        chunks[i] = chunk;
+        cprs[i] = nv ? (nv + chunk - 1) / chunk : 0;
+        const uint32_t* d_order = nullptr;
+        if (opts->schedule == GMK_SCHEDULE_ORDERED && j.task_cost) {
+            std::vector<uint32_t> order(g->nl);
+            std::iota(order.begin(), order.end(), 0u);
+            const float* cost = j.task_cost;
+            std::stable_sort(order.begin(), order.end(),
+                             [cost](uint32_t a, uint32_t b) { return cost[a] > cost[b]; });
+            if ((rc = grow((void**)&g->d_order, &g->order_bytes, 4ull * g->nl))) return rc;
+            CK(cudaMemcpyAsync(g->d_order, order.data(), 4ull * g->nl, cudaMemcpyHostToDevice,
+                               g0->stream));
+            d_order = g->d_order;
+        }
+        GraphTask& t = gt[i];
+        t.g = gmk::GraphView{g->d_off, g->d_adj, g->n, g->nl};
+        t.eh.slots = g->d_eh;
+        t.eh.bmask = g->eh_bmask;
+        t.k = j.k;
+        t.chunk = chunk;
+        t.n_roots = nroots;
+        t.root_base = j.root_begin;
+        t.root_order = d_order;
+        t.ctr = g->d_ctr;
+        t.root_nodes = nullptr;
+        if (j.root_nodes) {
+            if (!g->d_root_nodes) CK(cudaMalloc(&g->d_root_nodes, 8ull * g->nl));
+            CK(cudaMemsetAsync(g->d_root_nodes, 0, 8ull * g->nl, g0->stream));
+            t.root_nodes = g->d_root_nodes;
+        }
+        t.task_begin = n_tasks;
+        n_tasks += (unsigned long long)nroots * cprs[i];
+        CK(cudaMemsetAsync(g->d_ctr, 0, sizeof(Counters), g0->stream));
     }
+    const uint32_t nsh = opts->nshards ? opts->nshards : 1u, sh = opts->nshards ? opts->shard : 0u;
+    const unsigned long long my_tasks = n_tasks > sh ? (n_tasks - sh + nsh - 1) / nsh : 0;
+    if ((rc = grow((void**)&ws.d_graphs, &ws.graphs_bytes, sizeof(GraphTask) * ng))) return rc;
+    CK(cudaMemcpyAsync(ws.d_graphs, gt.data(), sizeof(GraphTask) * ng, cudaMemcpyHostToDevice,
+                       g0->stream));
+
     uint64_t out_words = 0;
     if (opts->emit) {
-        // the warp engine streams through two buffers of out_words each
+        // the warp engine streams through two buffers of out_words each, at
+        // least 128 words a warp (a smaller buffer would wind every round down
+        // after a few results and multiply the split tasks)
         out_words = opts->out_words ? opts->out_words : (warp ? (16ull << 20) : (64ull << 20));
+        if (warp) out_words = std::max<uint64_t>(out_words, workers * 128ull);
         if ((rc = grow((void**)&ws.d_out, &ws.out_bytes, out_words * 4ull * (warp ? 2 : 1))))
             return rc;
     }
@@ -667,8 +756,8 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
                                    : (opts->split_min_nodes ? opts->split_min_nodes : 64u);
     unsigned long long split_word_cap = 0, split_idx_cap = 0;
     if (warp) {   // split records: load balance, record-buffer draining, and round bookkeeping
-        split_word_cap = std::max<unsigned long long>(1ull << 22, workers * 4096ull);
-        split_idx_cap = std::max<unsigned long long>(1ull << 16, workers * 64ull);
+        split_word_cap = std::max<unsigned long long>(1ull << 22, workers * 8192ull);
+        split_idx_cap = std::max<unsigned long long>(1ull << 16, workers * 256ull);
         for (int b = 0; b < 2; ++b) {
             if ((rc = grow((void**)&ws.d_split_words[b], &ws.split_words_bytes[b], split_word_cap * 4)))
                 return rc;
@@ -676,46 +765,39 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
                 return rc;
         }
     }
-    CK(cudaMemsetAsync(g->d_ctr, 0, sizeof(Counters), g->stream));
-    gmk::GraphView gv{g->d_off, g->d_adj, g->n, g->nl};
     const unsigned grid = (unsigned)(threads / block);
     const unsigned long long watchdog_ns = (unsigned long long)opts->watchdog_ms * 1000000ull;
     const uint32_t pair_limit = opts->pair_limit ? opts->pair_limit : kDefaultPairLimit;
-    Counters h;
+    Counters h;          // launch-wide flags (graph 0's counters)
     unsigned long long tasks_total = 0, tasks_done = 0;
     uint32_t rounds = 0;
     int warp_emit_rc = GMK_OK;
-    CK(cudaEventRecord(g->ev0, g->stream));
+    CK(cudaEventRecord(g0->ev0, g0->stream));
     if (!warp) {
-        enumerate_kernel<<<grid, kBlock, 0, g->stream>>>(
-            gv, opts->k, g->d_ctr, ws.d_arena, arena_words, ws.d_sbuf, smax, pair_limit, n_tasks,
-            chunk, chunks_per_root, d_order, root_begin, opts->result_limit,
+        const GraphJob& j = jobs[0];
+        enumerate_kernel<<<grid, kBlock, 0, g0->stream>>>(
+            gt[0].g, j.k, g0->d_ctr, ws.d_arena, arena_words, ws.d_sbuf, smax, pair_limit, n_tasks,
+            chunks[0], cprs[0], gt[0].root_order, j.root_begin, opts->result_limit,
             opts->emit ? ws.d_out : nullptr, out_words, watchdog_ns, sh, nsh);
         CK(cudaGetLastError());
-        CK(cudaEventRecord(g->ev1, g->stream));
-        CK(cudaMemcpyAsync(&h, g->d_ctr, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
-        CK(cudaStreamSynchronize(g->stream));
+        CK(cudaEventRecord(g0->ev1, g0->stream));
+        CK(cudaMemcpyAsync(&h, g0->d_ctr, sizeof(h), cudaMemcpyDeviceToHost, g0->stream));
+        CK(cudaStreamSynchronize(g0->stream));
         tasks_total = my_tasks;
         tasks_done = std::min<unsigned long long>(h.tasks_done, my_tasks);
         rounds = 1;
     } else {
         WarpArgs a;
-        a.g = gv;
-        a.eh.slots = g->d_eh;
-        a.eh.bmask = g->eh_bmask;
-        a.k = opts->k;
-        a.ctr = g->d_ctr;
-        a.rc = g->d_rc;
+        a.single = gt[0];
+        a.graphs = static_cast<const GraphTask*>(ws.d_graphs);
+        a.n_graphs = (uint32_t)ng;
+        a.ctr = g0->d_ctr;
+        a.rc = g0->d_rc;
         a.arenas = ws.d_arena;
         a.arena_words = arena_words;
         a.sbuf = ws.d_sbuf;
         a.smax = smax;
         a.pair_limit = pair_limit;
-        a.chunk = chunk;
-        a.chunks_per_root = chunks_per_root;
-        a.root_order = d_order;
-        a.root_base = root_begin;
-        a.n_roots = root_end - root_begin;
         a.split_min_nodes = split_min;
         a.limit = opts->result_limit;
         a.out_buf = opts->emit ? ws.d_out : nullptr;
@@ -723,12 +805,6 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
         a.watchdog_ns = watchdog_ns;
         a.shard = sh;
         a.nshards = nsh;
-        a.root_nodes = nullptr;
-        if (opts->root_nodes) {
-            if (!g->d_root_nodes) CK(cudaMalloc(&g->d_root_nodes, 8ull * g->nl));
-            CK(cudaMemsetAsync(g->d_root_nodes, 0, 8ull * g->nl, g->stream));
-            a.root_nodes = g->d_root_nodes;
-        }
         // Record mode streams: each round writes one of two record buffers,
         // and while the next round runs the host hands the previous round's
         // records to the sink.  A round winds down (splits its tasks into the
@@ -748,25 +824,28 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
             a.cur_idx = ws.d_split_idx[cur];
             a.next.words = ws.d_split_words[cur ^ 1];
             a.next.idx = ws.d_split_idx[cur ^ 1];
-            a.next.used = &g->d_rc->next_used;
-            a.next.count = &g->d_rc->next_count;
-            a.next.count_fail = &g->d_rc->next_fail;
-            a.next.refused = &g->d_rc->split_refused;
+            a.next.used = &g0->d_rc->next_used;
+            a.next.count = &g0->d_rc->next_count;
+            a.next.count_fail = &g0->d_rc->next_fail;
+            a.next.refused = &g0->d_rc->split_refused;
             a.next.word_cap = split_word_cap;
             a.next.idx_cap = split_idx_cap;
             a.out_buf = opts->emit ? outb[round & 1] : nullptr;
-            CK(cudaMemsetAsync(g->d_rc, 0, sizeof(RoundCounters), g->stream));
-            CK(cudaMemsetAsync(&g->d_rc->out_fail, 0xFF, 2 * sizeof(unsigned long long), g->stream));
-            enumerate_warp_kernel<<<grid, kWBlock, 0, g->stream>>>(a);
+            CK(cudaMemsetAsync(g0->d_rc, 0, sizeof(RoundCounters), g0->stream));
+            CK(cudaMemsetAsync(&g0->d_rc->out_fail, 0xFF, 2 * sizeof(unsigned long long), g0->stream));
+            if (ng == 1)
+                enumerate_warp_kernel<false><<<grid, kWBlock, 0, g0->stream>>>(a);
+            else
+                enumerate_warp_kernel<true><<<grid, kWBlock, 0, g0->stream>>>(a);
             CK(cudaGetLastError());
             if (pending >= 0 && sink_rc == GMK_OK) {
-                sink_rc = deliver_records(g, outb[pending], pending_words, sink, user);
+                sink_rc = deliver_records(g0, outb[pending], pending_words, sink, user);
                 pending = -1;
             }
             RoundCounters r;
-            CK(cudaMemcpyAsync(&r, g->d_rc, sizeof(r), cudaMemcpyDeviceToHost, g->stream));
-            CK(cudaMemcpyAsync(&h, g->d_ctr, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
-            CK(cudaStreamSynchronize(g->stream));
+            CK(cudaMemcpyAsync(&r, g0->d_rc, sizeof(r), cudaMemcpyDeviceToHost, g0->stream));
+            CK(cudaMemcpyAsync(&h, g0->d_ctr, sizeof(h), cudaMemcpyDeviceToHost, g0->stream));
+            CK(cudaStreamSynchronize(g0->stream));
             ++rounds;
             tasks_total += a.queue_len;
             tasks_done += std::min<unsigned long long>(r.tasks_done, a.queue_len);
@@ -784,42 +863,49 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
                              why[r.split_refused >= 0 && r.split_refused <= 4 ? r.split_refused : 0];
             }
             if (h.error || h.stop || sink_rc != GMK_OK) break;
-            if (std::min({r.next_count, split_idx_cap, r.next_fail}) == 0 && root_next >= my_tasks)
-                break;
+            const unsigned long long next = std::min({r.next_count, split_idx_cap, r.next_fail});
+            if (next == 0 && root_next >= my_tasks) break;
             if (watchdog_ns) {
                 const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() -
                                                                 host_t0).count();
                 if (el * 1e9 > (double)watchdog_ns) { h.error = gmk::TASK_E_TIMEOUT; break; }
             }
-            n_records = std::min({r.next_count, split_idx_cap, r.next_fail});
+            n_records = next;
             cur ^= 1;
         }
-        CK(cudaEventRecord(g->ev1, g->stream));
-        CK(cudaStreamSynchronize(g->stream));
+        CK(cudaEventRecord(g0->ev1, g0->stream));
+        CK(cudaStreamSynchronize(g0->stream));
         if (pending >= 0 && sink_rc == GMK_OK && !h.error)
-            sink_rc = deliver_records(g, outb[pending], pending_words, sink, user);
+            sink_rc = deliver_records(g0, outb[pending], pending_words, sink, user);
         if (sink_rc < 0 && sink_rc != GMK_E_SINK) return sink_rc;
         if (sink_rc == GMK_E_SINK) warp_emit_rc = GMK_E_SINK;
-        if (opts->root_nodes) {
+        for (size_t i = 0; i < ng; ++i) {
+            if (!jobs[i].root_nodes) continue;
+            gmk_graph* g = jobs[i].g;
             std::vector<unsigned long long> rn(g->nl);
             CK(cudaMemcpy(rn.data(), g->d_root_nodes, 8ull * g->nl, cudaMemcpyDeviceToHost));
-            for (uint32_t i = 0; i < g->nl; ++i) opts->root_nodes[i] += rn[i];
+            for (uint32_t v = 0; v < g->nl; ++v) jobs[i].root_nodes[v] += rn[v];
         }
     }
     float ms = 0.f;
-    CK(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
-
-    out->count = opts->result_limit ? std::min<unsigned long long>(h.count, opts->result_limit) : h.count;
-    out->hash_sum = h.hash_sum;
-    out->hash_xor = h.hash_xor;
-    out->nodes = h.nodes;
-    out->algo_bytes = 4ull * h.work;
-    out->tasks = tasks_total;
-    out->tasks_done = tasks_done;
-    out->kernel_ms = ms;
-    out->truncated = opts->result_limit && h.count >= opts->result_limit;
-    out->threads = (uint32_t)threads;
-    out->rounds = rounds;
+    CK(cudaEventElapsedTime(&ms, g0->ev0, g0->ev1));
+    for (size_t i = 0; i < ng; ++i) {
+        Counters hc = h;
+        if (i) CK(cudaMemcpy(&hc, jobs[i].g->d_ctr, sizeof(hc), cudaMemcpyDeviceToHost));
+        gmk_stats* out = outs + i;
+        out->count = opts->result_limit ? std::min<unsigned long long>(hc.count, opts->result_limit)
+                                        : hc.count;
+        out->hash_sum = hc.hash_sum;
+        out->hash_xor = hc.hash_xor;
+        out->nodes = hc.nodes;
+        out->algo_bytes = 4ull * hc.work;
+        out->tasks = tasks_total;
+        out->tasks_done = tasks_done;
+        out->kernel_ms = ms;
+        out->truncated = opts->result_limit && hc.count >= opts->result_limit;
+        out->threads = (uint32_t)threads;
+        out->rounds = rounds;
+    }
     switch (h.error) {
         case gmk::TASK_OK: break;
         case gmk::TASK_E_ARENA: return GMK_E_ARENA;
@@ -846,6 +932,66 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
         }
     }
     return GMK_OK;
+}
+
+int check_opts(const gmk_opts* opts) {
+    if (opts->k < 1 || opts->k > 15) return GMK_E_INVAL;
+    if (opts->schedule < GMK_SCHEDULE_PLAIN || opts->schedule > GMK_SCHEDULE_ORDERED)
+        return GMK_E_INVAL;
+    if (opts->nshards && opts->shard >= opts->nshards) return GMK_E_INVAL;
+    if (opts->engine != GMK_ENGINE_WARP && opts->engine != GMK_ENGINE_THREAD) return GMK_E_INVAL;
+    return GMK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user, gmk_stats* out) {
+    if (!g || !opts || !out) return GMK_E_INVAL;
+    if (int rc = check_opts(opts)) return rc;
+    if (opts->emit && !sink) return GMK_E_INVAL;
+    if (opts->schedule == GMK_SCHEDULE_ORDERED && !opts->task_cost) return GMK_E_INVAL;
+    if (opts->root_nodes && opts->engine != GMK_ENGINE_WARP) return GMK_E_INVAL;
+    const uint32_t root_end = opts->root_end ? opts->root_end : g->nl;
+    if (root_end > g->nl || opts->root_begin > root_end) return GMK_E_INVAL;
+    std::memset(out, 0, sizeof(*out));
+    CK(cudaSetDevice(g->device));
+    if (g->nl == 0 || g->n == g->nl || opts->root_begin == root_end) return GMK_OK;   // nothing to do
+    std::vector<GraphJob> jobs{{g, opts->k, opts->root_begin, root_end, opts->task_cost,
+                                opts->root_nodes}};
+    return run_jobs(jobs, opts, sink, user, out);
+}
+
+int gmk_enumerate_batch(gmk_graph* const* graphs, uint32_t n_graphs, const uint32_t* ks,
+                        const float* const* task_costs, const gmk_opts* opts, gmk_stats* outs) {
+    if (!graphs || !opts || !outs || n_graphs == 0) return GMK_E_INVAL;
+    if (int rc = check_opts(opts)) return rc;
+    if (opts->engine != GMK_ENGINE_WARP || opts->emit || opts->result_limit || opts->root_nodes ||
+        opts->root_begin || opts->root_end || (opts->nshards > 1))
+        return GMK_E_INVAL;
+    std::memset(outs, 0, sizeof(gmk_stats) * n_graphs);
+    std::vector<GraphJob> jobs;
+    std::vector<uint32_t> slot;   // jobs[i] is graphs[slot[i]]
+    for (uint32_t i = 0; i < n_graphs; ++i) {
+        gmk_graph* g = graphs[i];
+        if (!g || g->device != graphs[0]->device) return GMK_E_INVAL;
+        const uint32_t k = ks ? ks[i] : opts->k;
+        if (k < 1 || k > 15) return GMK_E_INVAL;
+        if (opts->schedule == GMK_SCHEDULE_ORDERED && (!task_costs || !task_costs[i]))
+            return GMK_E_INVAL;
+        for (uint32_t j = 0; j < i; ++j)
+            if (graphs[j] == g) return GMK_E_INVAL;   // each graph's counters are its own
+        if (g->nl == 0 || g->n == g->nl) continue;    // a side is empty: no k-biplex
+        jobs.push_back({g, k, 0, g->nl, task_costs ? task_costs[i] : nullptr, nullptr});
+        slot.push_back(i);
+    }
+    if (jobs.empty()) return GMK_OK;
+    CK(cudaSetDevice(graphs[0]->device));
+    std::vector<gmk_stats> tmp(jobs.size());
+    const int rc = run_jobs(jobs, opts, nullptr, nullptr, tmp.data());
+    for (size_t i = 0; i < jobs.size(); ++i) outs[slot[i]] = tmp[i];
+    return rc;
 }
 
 // ---------------------------------------------------------------- learned schedule

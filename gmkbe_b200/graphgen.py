@@ -213,6 +213,30 @@ WORKLOADS = {
 }
 
 
+def mixed_batch(n_graphs: int = 64, seed0: int = 100, size_lo: int = 1_000,
+                size_hi: int = 50_000, deg_lo: float = 5.0, deg_hi: float = 30.0,
+                gamma: float = 2.1) -> tuple[list[Graph], list[int]]:
+    """A batch of uneven graphs and their k: graph i (seed seed0 + i) has |U|
+    and |V| log-uniform in [size_lo, size_hi], average U-side degree uniform in
+    [deg_lo, deg_hi] (capped by |V|), Erdos-Renyi for even i and Chung-Lu with
+    exponent gamma for odd i, and k drawn from {1, 2, 3}."""
+    graphs, ks = [], []
+    for i in range(n_graphs):
+        seed = seed0 + i
+        rng = np.random.Generator(np.random.PCG64(seed))
+        nu = int(round(np.exp(rng.uniform(np.log(size_lo), np.log(size_hi)))))
+        nv = int(round(np.exp(rng.uniform(np.log(size_lo), np.log(size_hi)))))
+        deg = min(float(rng.uniform(deg_lo, deg_hi)), 0.9 * nv)
+        k = int(rng.integers(1, 4))
+        if i % 2 == 0:
+            g = erdos_renyi(nu, nv, deg / nv, seed)
+        else:
+            g = chung_lu(nu, nv, max(1, int(deg * nu)), gamma, seed)
+        graphs.append(g)
+        ks.append(k)
+    return graphs, ks
+
+
 def make_workload(name: str) -> Graph:
     w = WORKLOADS[name]
     if w["kind"] == "er":

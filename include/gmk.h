@@ -136,6 +136,18 @@ void gmk_opts_default(gmk_opts* o);
 int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
                   gmk_stats* out);
 
+/* No counterpart in the reference (one graph per gmkbpe process).  Enumerates
+ * n_graphs graphs, all loaded on the same device, in one run of persistent
+ * launches: the root tasks of every graph share one device work queue, so
+ * many small or uneven graphs keep the GPU busy together.  ks[i] is graph i's
+ * k (NULL: opts->k for all); with GMK_SCHEDULE_ORDERED, task_costs[i] gives
+ * graph i's per-root costs.  Full enumeration only: opts must have emit = 0,
+ * result_limit = 0, no root range, no root_nodes, no sharding, and the warp
+ * engine.  outs[i] receives graph i's count and set hash (kernel_ms, rounds
+ * and tasks are those of the whole batch).  A graph may appear only once. */
+int gmk_enumerate_batch(gmk_graph* const* graphs, uint32_t n_graphs, const uint32_t* ks,
+                        const float* const* task_costs, const gmk_opts* opts, gmk_stats* outs);
+
 /* No counterpart in the reference, which has no resume (its "checkpoints" are
  * result-count milestones, src/main.cu:1753-1761).  Runs gmk_enumerate over
  * consecutive batches of `batch_roots` roots (0 = automatic) and, after each

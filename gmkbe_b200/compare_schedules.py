@@ -33,15 +33,24 @@ from .api import Graph, enumerate_batch
 
 GOLDEN = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tests",
                       "golden")
-CASES = [("crime", 1), ("er200", 1), ("cl20k_sub", 1), ("southernwomen", 3), ("er60", 2)]
+CASES = [("er200", 1), ("cl20k_sub", 1), ("southernwomen", 3), ("er60", 2), ("crime", 1)]
+WATCHDOG_MS = 30_000   # a schedule that has not finished by then is reported as such
 
 
-def _timed(g: Graph, reps: int = 3, **kw):
-    best, st = None, None
-    for _ in range(reps):
-        st = g.enumerate(**kw)
-        best = st.kernel_ms if best is None else min(best, st.kernel_ms)
-    return best, st
+def _timed(g: Graph, **kw):
+    """(device ms, stats) of one run, or (None, None) when the watchdog ended it."""
+    from .api import GmkError
+    try:
+        st = g.enumerate(watchdog_ms=WATCHDOG_MS, **kw)
+    except GmkError as e:
+        if e.code == -8:
+            return None, None
+        raise
+    return st.kernel_ms, st
+
+
+def _ratio(a, b):
+    return None if a is None or b is None else a / b
 
 
 def _train_model(k: int) -> L.SubtreeModel:
@@ -63,23 +72,29 @@ def full_enumerations() -> list[dict]:
         with Graph.load(os.path.join(GOLDEN, f"{name}.graph.bin")) as g:
             if k not in models:
                 models[k] = _train_model(k)
-            t_plain, s_plain = _timed(g, k=k, schedule="plain")
             t_batch, s_batch = _timed(g, k=k, schedule="batched")
-            nodes = L.subtree_nodes(g, k)
             cost = L.predicted_costs(models[k], g, k)
             t_learn, s_learn = _timed(g, k=k, schedule="ordered", task_cost=cost)
-            same = s_plain.summary() == s_batch.summary() == s_learn.summary()
-            out.append({"graph": name, "k": k, "results": s_plain.count,
-                        "plain_ms": t_plain, "batched_ms": t_batch, "learned_ms": t_learn,
-                        "batched_speedup": t_plain / t_batch, "learned_speedup": t_plain / t_learn,
-                        "rounds_batched": s_batch.rounds, "same_set": same,
-                        "spearman": L.spearman(cost, nodes),
-                        "mean_relative_error": L.mean_relative_error(cost, nodes)})
+            t_plain, s_plain = _timed(g, k=k, schedule="plain")
+            sums = {s.summary() for s in (s_plain, s_batch, s_learn) if s is not None}
+            row = {"graph": name, "k": k, "results": (s_batch or s_plain).count if (s_batch or s_plain) else None,
+                   "plain_ms": t_plain, "batched_ms": t_batch, "learned_ms": t_learn,
+                   "batched_speedup": _ratio(t_plain, t_batch),
+                   "learned_speedup": _ratio(t_plain, t_learn),
+                   "rounds_batched": s_batch.rounds if s_batch else None,
+                   "same_set": len(sums) == 1, "watchdog_ms": WATCHDOG_MS}
+            if s_plain is not None:
+                nodes = L.subtree_nodes(g, k, watchdog_ms=WATCHDOG_MS)
+                row["spearman"] = L.spearman(cost, nodes)
+                row["mean_relative_error"] = L.mean_relative_error(cost, nodes)
+            print(json.dumps(row), flush=True)
+            out.append(row)
     return out
 
 
 def mixed_batch() -> dict:
     gs, ks = gg.mixed_batch(64, 100, size_lo=6, size_hi=40, deg_lo=1.5, deg_hi=3.0)
+    from .api import GmkError
     pairs = [(g, k) for g, k in zip(gs, ks) if g.n_left not in (0, g.n)]
     dgs = [Graph.from_graph(g) for g, _ in pairs]
     ks = [k for _, k in pairs]
@@ -88,10 +103,18 @@ def mixed_batch() -> dict:
         t0 = time.perf_counter()
         batch = enumerate_batch(dgs, ks)
         wall_batch = time.perf_counter() - t0
-        seq_ms, seq_wall, same = 0.0, 0.0, True
+        seq_ms, seq_wall, same, unfinished = 0.0, 0.0, True, 0
         for dg, k, st in zip(dgs, ks, batch):
             t0 = time.perf_counter()
-            s = dg.enumerate(k=k, schedule="plain")
+            try:
+                s = dg.enumerate(k=k, schedule="plain", watchdog_ms=WATCHDOG_MS)
+            except GmkError as e:
+                if e.code != -8:
+                    raise
+                unfinished += 1
+                seq_ms += WATCHDOG_MS
+                seq_wall += time.perf_counter() - t0
+                continue
             seq_wall += time.perf_counter() - t0
             seq_ms += s.kernel_ms
             same &= s.summary() == st.summary()
@@ -101,6 +124,7 @@ def mixed_batch() -> dict:
                 "one_launch_per_graph_wall_s": seq_wall,
                 "speedup_device": seq_ms / batch[0].kernel_ms,
                 "speedup_wall": seq_wall / wall_batch, "same_sets": same,
+                "plain_runs_unfinished_at_watchdog": unfinished,
                 "batch_results_per_s": total / (batch[0].kernel_ms / 1e3)}
     finally:
         for dg in dgs:
@@ -111,8 +135,9 @@ def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--json", help="also write the results here")
     a = ap.parse_args(argv)
-    res = {"full_enumeration": full_enumerations(), "mixed_batch": mixed_batch()}
-    print(json.dumps(res, indent=1))
+    res = {"full_enumeration": full_enumerations()}
+    res["mixed_batch"] = mixed_batch()
+    print(json.dumps(res["mixed_batch"]), flush=True)
     if a.json:
         with open(a.json, "w") as f:
             json.dump(res, f, indent=1)

@@ -39,10 +39,10 @@ def root_features(g: Graph, k: int) -> np.ndarray:
 
 
 def subtree_nodes(g: Graph, k: int, **kw) -> np.ndarray:
-    """Search nodes of every root task, logged by a plain-schedule run (one
-    task per root, no splitting)."""
+    """Search nodes of every root task, logged by a batched run (split records
+    carry their root, so the log is per root whatever the schedule)."""
     nodes = np.zeros(g.n_left, np.uint64)
-    g.enumerate(k=k, schedule="plain", root_nodes=nodes, **kw)
+    g.enumerate(k=k, schedule="batched", root_nodes=nodes, **kw)
     return nodes
 
 

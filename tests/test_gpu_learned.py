@@ -70,8 +70,11 @@ def test_features_and_subtree_log_on_the_gpu():
         deg = g.degree()[: g.n_left]
         assert np.allclose(f[:, 2], np.log1p(deg), atol=2e-3 * np.log1p(deg).max())
         nodes = L.subtree_nodes(dg, 1)
-        total = dg.enumerate(k=1, schedule="plain")
+        total = dg.enumerate(k=1, schedule="batched")   # same chunking, same tree
         assert nodes.sum() == total.nodes and (nodes > 0).all()
+        plain = np.zeros(g.n_left, np.uint64)
+        st = dg.enumerate(k=1, schedule="plain", root_nodes=plain)
+        assert plain.sum() == st.nodes
 
 
 def test_learned_order_ranks_roots_and_keeps_the_set():

@@ -154,6 +154,9 @@ struct Ctx {
     uint32_t cap;
     uint32_t* sid;
     uint32_t* smc;
+    uint32_t* smask;       // smask[i]: members below i that member i missed, bit j = member j
+                           // (valid for mask_base <= i <= 32)
+    uint32_t mask_base;    // members restored from a split record carry no mask
     uint32_t smax;
     uint32_t ns;
     U2 nss;                                      // |S| per side
@@ -220,7 +223,7 @@ __device__ uint32_t compat_lane(Ctx& t, uint32_t w) {
 // because of c go to t.sat (first kSatCap, in S order), their count to *nsat.
 __device__ uint32_t push_member(Ctx& t, uint32_t c, uint32_t* nsat_out) {
     const int s = side_of(t.g, c);
-    uint32_t miss = 0, nsat = 0;
+    uint32_t miss = 0, nsat = 0, mask0 = 0;
     for (uint32_t base = 0; base < t.ns; base += 32) {
         const uint32_t i = base + t.lane;
         bool nm = false, sat = false;
@@ -234,7 +237,9 @@ __device__ uint32_t push_member(Ctx& t, uint32_t c, uint32_t* nsat_out) {
                 sat = v == t.k;
             }
         }
-        miss += __popc(__ballot_sync(kFull, nm));
+        const uint32_t nmask = __ballot_sync(kFull, nm);
+        if (base == 0) mask0 = nmask;
+        miss += __popc(nmask);
         const uint32_t sm = __ballot_sync(kFull, sat);
         if (sat) {
             const uint32_t r = nsat + __popc(sm & lanemask_lt());
@@ -245,6 +250,7 @@ __device__ uint32_t push_member(Ctx& t, uint32_t c, uint32_t* nsat_out) {
     if (t.lane == 0) {
         t.sid[t.ns] = c;
         t.smc[t.ns] = miss;
+        t.smask[t.ns] = mask0;
     }
     __syncwarp();
     t.ns++;
@@ -258,11 +264,17 @@ __device__ void pop_member(Ctx& t) {
     t.ns--;
     const int s = side_of(t.g, c);
     t.nss.set(s, t.nss.get(s) - 1);
-    for (uint32_t base = 0; base < t.ns; base += 32) {
-        const uint32_t i = base + t.lane;
-        if (i < t.ns) {
-            const uint32_t m = t.sid[i];
-            if (side_of(t.g, m) != s && !adj_test(t, c, m)) t.smc[i]--;
+    if (t.ns <= 32 && t.ns >= t.mask_base) {
+        // the members c missed, as recorded when c was pushed
+        const uint32_t mask = t.smask[t.ns];
+        if (t.lane < t.ns && ((mask >> t.lane) & 1u)) t.smc[t.lane]--;
+    } else {
+        for (uint32_t base = 0; base < t.ns; base += 32) {
+            const uint32_t i = base + t.lane;
+            if (i < t.ns) {
+                const uint32_t m = t.sid[i];
+                if (side_of(t.g, m) != s && !adj_test(t, c, m)) t.smc[i]--;
+            }
         }
     }
     __syncwarp();
@@ -474,6 +486,7 @@ __device__ bool outsider_addable_mixed(Ctx& t, int s, uint32_t lo, const uint32_
 
 // Counts (and in record mode writes) the result S u list0 u list1.  Returns
 // false only in record mode when the record found no room.
+template <bool kRec>
 __device__ bool emit(Ctx& t, const Outputs& o, const uint32_t* l0, uint32_t n0, const uint32_t* l1,
                      uint32_t n1) {
     unsigned long long a = 0, b = 0;
@@ -492,7 +505,7 @@ __device__ bool emit(Ctx& t, const Outputs& o, const uint32_t* l0, uint32_t n0, 
     a = warp_sum64(a);
     b = warp_sum64(b);
     const uint32_t nx = t.nss.a + n0, ny = t.nss.b + n1;
-    if (o.out_buf) {
+    if (kRec) {
         // record mode: room first, then the count (exact limit).  A record
         // that finds no room is not counted: the caller defers the node to
         // the next round, after the host has drained the buffer.
@@ -753,6 +766,7 @@ struct ChildReq {
 
 // Warp form of enter_node (enum_core.cuh).  ENTER_PUSHED: a forced candidate
 // was found; *req describes the child to build.
+template <bool kRec>
 __device__ int enter_node(Ctx& t, const Outputs& o, uint32_t cur, ChildReq* req) {
     const GraphView& g = t.g;
     const Hdr f = read_hdr(t.arena + cur);
@@ -812,7 +826,7 @@ __device__ int enter_node(Ctx& t, const Outputs& o, uint32_t cur, ChildReq* req)
             const bool addable = outsider_addable(t, l0, n0, l1, n1, tot);
             if (biplex) {
                 // S u C is a k-biplex: the only leaf that can be maximal
-                if (!addable && !emit(t, o, l0, n0, l1, n1)) return ENTER_DEFER;
+                if (!addable && !emit<kRec>(t, o, l0, n0, l1, n1)) return ENTER_DEFER;
                 return ENTER_DONE;
             }
             if (addable) return ENTER_DONE;
@@ -1042,6 +1056,7 @@ __device__ __forceinline__ bool draining(const RunLimits& lim) {
 
 // Depth-first search from the frame at arena offset 0; returns the nodes it
 // entered.
+template <bool kRec>
 __device__ unsigned long long run_dfs(Ctx& t, const Outputs& o, uint32_t first,
                                       const SplitBuf* sb, const RunLimits& lim) {
     uint32_t cur = 0;
@@ -1058,7 +1073,7 @@ __device__ unsigned long long run_dfs(Ctx& t, const Outputs& o, uint32_t first,
                 hungry = may_split && task_nodes >= 1 &&
                          ((lim.split_min_nodes && task_nodes >= lim.split_min_nodes &&
                            *(volatile const unsigned long long*)lim.queue >= lim.queue_len) ||
-                          draining(lim));
+                          (kRec && draining(lim)));
             }
             stop = bcast(stop); late = bcast(late); hungry = bcast(hungry);
             if (stop) break;
@@ -1077,8 +1092,8 @@ __device__ unsigned long long run_dfs(Ctx& t, const Outputs& o, uint32_t first,
             __syncwarp();
             t.nodes++;
             task_nodes++;
-            const int r = enter_node(t, o, cur, &req);
-            if (r == ENTER_DEFER) {
+            const int r = enter_node<kRec>(t, o, cur, &req);
+            if (kRec && r == ENTER_DEFER) {
                 // re-enter this node next round, after the host drained the buffer
                 set_word(t, cur + F_FLAGS, flags);
                 t.nodes--;
@@ -1106,9 +1121,11 @@ __device__ unsigned long long run_dfs(Ctx& t, const Outputs& o, uint32_t first,
 }
 
 // Root task: x in U with its first-level children y in [first, last).
+template <bool kRec>
 __device__ unsigned long long run_root(Ctx& t, const Outputs& o, uint32_t root, uint32_t first,
                                        uint32_t last, const SplitBuf* sb, const RunLimits& lim) {
     t.ns = 0; t.nss.a = t.nss.b = 0;
+    t.mask_base = 0;
     push_member(t, root, nullptr);
     Hdr h;
     h.ns = 1; h.flags = FL_G0 | FL_G1 | FL_ROOT;
@@ -1124,10 +1141,11 @@ __device__ unsigned long long run_root(Ctx& t, const Outputs& o, uint32_t root, 
         }
     if (t.lane == 0) write_hdr(t.arena, h);
     __syncwarp();
-    return run_dfs(t, o, first, sb, lim);
+    return run_dfs<kRec>(t, o, first, sb, lim);
 }
 
 // Resumed task: a frame written by split_path (its S starts with the root).
+template <bool kRec>
 __device__ unsigned long long run_record(Ctx& t, const Outputs& o, const uint32_t* r,
                                          const SplitBuf* sb, const RunLimits& lim) {
     const uint32_t ns = r[0], c0 = r[1], c1 = r[2];
@@ -1147,6 +1165,7 @@ __device__ unsigned long long run_record(Ctx& t, const Outputs& o, const uint32_
         nv += __popc(__ballot_sync(kFull, isv));
     }
     t.ns = ns; t.nss.b = nv; t.nss.a = ns - nv;
+    t.mask_base = ns;
     const uint32_t* fr = rs + 2 * ns;
     Hdr h = read_hdr(fr);
     h.off.a = F_WORDS;
@@ -1157,7 +1176,7 @@ __device__ unsigned long long run_record(Ctx& t, const Outputs& o, const uint32_
     for (uint32_t i = t.lane; i < 2 * (c0 + c1); i += 32) t.arena[F_WORDS + i] = lr[i];
     if (t.lane == 0) write_hdr(t.arena, h);
     __syncwarp();
-    return run_dfs(t, o, 0, sb, lim);
+    return run_dfs<kRec>(t, o, 0, sb, lim);
 }
 
 }  // namespace warp

@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <new>
 #include <numeric>
@@ -171,7 +172,9 @@ __device__ __forceinline__ const GraphTask& use_graph(const WarpArgs& a, uint32_
     return G;
 }
 
-template <bool kBatch>
+// kBatch: several graphs per launch; kRec: results written as records (the
+// count-only instantiation carries none of the record and drain code).
+template <bool kBatch, bool kRec>
 __global__ void __launch_bounds__(kWBlock, GMK_WARP_MIN_BLOCKS) enumerate_warp_kernel(const WarpArgs a) {
     __shared__ uint32_t s_sat[kWarpsPerBlock][gmk::kSatCap];
     __shared__ uint32_t s_src[kWarpsPerBlock][gmk::warp::kSrcCap];
@@ -199,7 +202,8 @@ __global__ void __launch_bounds__(kWBlock, GMK_WARP_MIN_BLOCKS) enumerate_warp_k
     Ctx t;
     use_graph<kBatch>(a, 0, t, o);
     t.arena = a.arenas + wid * a.arena_words; t.cap = a.arena_words;
-    t.sid = a.sbuf + wid * 2ull * a.smax; t.smc = t.sid + a.smax; t.smax = a.smax;
+    t.sid = a.sbuf + wid * 3ull * a.smax; t.smc = t.sid + a.smax; t.smask = t.smc + a.smax;
+    t.smax = a.smax; t.mask_base = 0;
     t.ns = 0; t.nss.a = t.nss.b = 0;
     t.scan_limit = a.pair_limit; t.err = 0;
     t.cnt = t.hsum = t.hxor = t.nodes = 0; t.work = 0;
@@ -217,7 +221,7 @@ __global__ void __launch_bounds__(kWBlock, GMK_WARP_MIN_BLOCKS) enumerate_warp_k
         if (lane == 0) {
             stop = gmk::load_flag(o.stop);
             if (!stop) {
-                if (!draining(lim)) {
+                if (!(kRec && draining(lim))) {
                     j = atomicAdd(&a.rc->next_task, 1ull);
                 } else {
                     // winding down: take only split records (they must all be
@@ -260,14 +264,14 @@ __global__ void __launch_bounds__(kWBlock, GMK_WARP_MIN_BLOCKS) enumerate_warp_k
             const uint32_t first = t.g.nl + c * G.chunk;
             const unsigned long long end = (unsigned long long)first + G.chunk;
             const uint32_t last = end < t.g.n ? (uint32_t)end : t.g.n;
-            const unsigned long long nodes = run_root(t, o, root, first, last, sb, lim);
+            const unsigned long long nodes = run_root<kRec>(t, o, root, first, last, sb, lim);
             if (G.root_nodes && lane == 0) atomicAdd(G.root_nodes + root, nodes);
         } else {
             const uint32_t* rec = a.cur_words + a.cur_idx[j];
             const GraphTask& G = use_graph<kBatch>(a, kBatch ? rec[3] : 0u, t, o);
             // a round that winds down hands its queued records on unchanged
-            if (!(sb && draining(lim) && forward_record(t, *sb, rec))) {
-                const unsigned long long nodes = run_record(t, o, rec, sb, lim);
+            if (!(kRec && sb && draining(lim) && forward_record(t, *sb, rec))) {
+                const unsigned long long nodes = run_record<kRec>(t, o, rec, sb, lim);
                 if (G.root_nodes && lane == 0)
                     atomicAdd(G.root_nodes + rec[gmk::warp::kRecHeader], nodes);
             }
@@ -325,6 +329,7 @@ struct gmk_graph {
     uint64_t adj_len = 0;
     uint64_t fingerprint = 0;   // hash of the CSR (checkpoint identity)
     uint32_t max_degree = 0;
+    uint32_t max_degree_side[2] = {0, 0};   // U side, V side
     uint32_t* d_off = nullptr;
     uint32_t* d_adj = nullptr;
     Counters* d_ctr = nullptr;
@@ -332,6 +337,7 @@ struct gmk_graph {
     size_t order_bytes = 0;
     unsigned long long* d_eh = nullptr;   // edge hash: buckets of 4 keys
     unsigned long long eh_bmask = 0;
+    size_t eh_bytes = 0;
     unsigned long long* d_root_nodes = nullptr;   // per-root node log (on demand)
     __half* d_feat = nullptr;                     // root features (on demand)
     RoundCounters* d_rc = nullptr;
@@ -386,6 +392,77 @@ int grow(void** p, size_t* have, size_t need) {
     return GMK_OK;
 }
 
+// Per-device cache of graph buffers, streams and events.  Loading and freeing
+// graphs one after another (a service handling many requests, the bench's
+// end-to-end loop) then reuses device memory instead of paying cudaMalloc /
+// cudaFree (which synchronises the device) and stream creation every time.
+// At most kPoolCap bytes stay cached per device; the rest is freed.
+constexpr size_t kPoolCap = 2ull << 30;
+struct DevPool {
+    std::mutex mu;
+    std::multimap<size_t, void*> blocks;   // size -> block
+    size_t cached = 0;
+    std::vector<cudaStream_t> streams;
+    std::vector<cudaEvent_t> events;
+};
+DevPool g_pool[64];
+
+size_t pool_round(size_t bytes) { return (std::max<size_t>(bytes, 1) + 255) / 256 * 256; }
+
+cudaError_t pool_alloc(int dev, void** p, size_t bytes) {
+    bytes = pool_round(bytes);
+    {
+        DevPool& pl = g_pool[dev];
+        std::lock_guard<std::mutex> lock(pl.mu);
+        auto it = pl.blocks.find(bytes);   // exact sizes only: graph buffers repeat exactly
+        if (it != pl.blocks.end()) {
+            *p = it->second;
+            pl.cached -= it->first;
+            pl.blocks.erase(it);
+            return cudaSuccess;
+        }
+    }
+    return cudaMalloc(p, bytes);
+}
+
+void pool_free(int dev, void* p, size_t bytes) {
+    if (!p) return;
+    bytes = pool_round(bytes);
+    DevPool& pl = g_pool[dev];
+    std::lock_guard<std::mutex> lock(pl.mu);
+    if (pl.cached + bytes <= kPoolCap) {
+        pl.blocks.emplace(bytes, p);
+        pl.cached += bytes;
+    } else {
+        cudaFree(p);
+    }
+}
+
+cudaError_t pool_stream(int dev, cudaStream_t* s) {
+    {
+        DevPool& pl = g_pool[dev];
+        std::lock_guard<std::mutex> lock(pl.mu);
+        if (!pl.streams.empty()) { *s = pl.streams.back(); pl.streams.pop_back(); return cudaSuccess; }
+    }
+    return cudaStreamCreateWithFlags(s, cudaStreamNonBlocking);
+}
+
+cudaError_t pool_event(int dev, cudaEvent_t* ev) {
+    {
+        DevPool& pl = g_pool[dev];
+        std::lock_guard<std::mutex> lock(pl.mu);
+        if (!pl.events.empty()) { *ev = pl.events.back(); pl.events.pop_back(); return cudaSuccess; }
+    }
+    return cudaEventCreate(ev);
+}
+
+void pool_return(int dev, cudaStream_t s, cudaEvent_t ev) {
+    DevPool& pl = g_pool[dev];
+    std::lock_guard<std::mutex> lock(pl.mu);
+    if (s) pl.streams.push_back(s);
+    if (ev) pl.events.push_back(ev);
+}
+
 // Copies `words` record words from the device and hands every record to the
 // sink (ids sorted per side).  Runs on the graph's copy stream, so it overlaps
 // the round the enumeration stream is running.
@@ -405,18 +482,22 @@ int upload(const uint32_t* off, const uint32_t* adj, uint32_t n, uint32_t nl, in
     gmk_graph* g = new (std::nothrow) gmk_graph();
     if (!g) return GMK_E_NOMEM;
     g->device = device; g->n = n; g->nl = nl; g->adj_len = off[n];
-    for (uint32_t v = 0; v < n; ++v)
-        if (off[v + 1] > off[v]) g->max_degree = std::max(g->max_degree, off[v + 1] - off[v]);
+    for (uint32_t v = 0; v < n; ++v) {
+        const uint32_t d = off[v + 1] > off[v] ? off[v + 1] - off[v] : 0u;
+        g->max_degree = std::max(g->max_degree, d);
+        uint32_t& side_max = g->max_degree_side[v < nl ? 0 : 1];
+        side_max = std::max(side_max, d);
+    }
     auto bail = [&](int code) { gmk_graph_free(g); return code; };
     cudaError_t e;
-    if ((e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking)) != cudaSuccess ||
-        (e = cudaStreamCreateWithFlags(&g->copy_stream, cudaStreamNonBlocking)) != cudaSuccess)
+    if ((e = pool_stream(device, &g->stream)) != cudaSuccess ||
+        (e = pool_stream(device, &g->copy_stream)) != cudaSuccess)
         return bail(cuda_fail(e, "cudaStreamCreate"));
-    if ((e = cudaEventCreate(&g->ev0)) != cudaSuccess || (e = cudaEventCreate(&g->ev1)) != cudaSuccess)
+    if ((e = pool_event(device, &g->ev0)) != cudaSuccess || (e = pool_event(device, &g->ev1)) != cudaSuccess)
         return bail(cuda_fail(e, "cudaEventCreate"));
-    if ((e = cudaMalloc(&g->d_off, sizeof(uint32_t) * (n + 1ull))) != cudaSuccess)
+    if ((e = pool_alloc(device, (void**)&g->d_off, sizeof(uint32_t) * (n + 1ull))) != cudaSuccess)
         return bail(cuda_fail(e, "cudaMalloc(offsets)"));
-    if ((e = cudaMalloc(&g->d_adj, sizeof(uint32_t) * std::max<uint64_t>(1, g->adj_len))) != cudaSuccess)
+    if ((e = pool_alloc(device, (void**)&g->d_adj, sizeof(uint32_t) * std::max<uint64_t>(1, g->adj_len))) != cudaSuccess)
         return bail(cuda_fail(e, "cudaMalloc(adj)"));
     if ((e = cudaMemcpyAsync(g->d_off, off, sizeof(uint32_t) * (n + 1ull), cudaMemcpyHostToDevice,
                              g->stream)) != cudaSuccess)
@@ -424,9 +505,9 @@ int upload(const uint32_t* off, const uint32_t* adj, uint32_t n, uint32_t nl, in
     if (g->adj_len && (e = cudaMemcpyAsync(g->d_adj, adj, sizeof(uint32_t) * g->adj_len,
                                            cudaMemcpyHostToDevice, g->stream)) != cudaSuccess)
         return bail(cuda_fail(e, "H2D adj"));
-    if ((e = cudaMalloc(&g->d_ctr, sizeof(Counters))) != cudaSuccess)
+    if ((e = pool_alloc(device, (void**)&g->d_ctr, sizeof(Counters))) != cudaSuccess)
         return bail(cuda_fail(e, "cudaMalloc(counters)"));
-    if ((e = cudaMalloc(&g->d_rc, sizeof(RoundCounters))) != cudaSuccess)
+    if ((e = pool_alloc(device, (void**)&g->d_rc, sizeof(RoundCounters))) != cudaSuccess)
         return bail(cuda_fail(e, "cudaMalloc(round counters)"));
     // check the CSR on the device before anything reads it as a graph
     {
@@ -452,7 +533,8 @@ int upload(const uint32_t* off, const uint32_t* adj, uint32_t n, uint32_t nl, in
         while (buckets * 2 < edges) buckets <<= 1;
         g->eh_bmask = buckets - 1;
         const size_t bytes = buckets * 4 * sizeof(unsigned long long);
-        if ((e = cudaMalloc(&g->d_eh, bytes)) != cudaSuccess)
+        g->eh_bytes = bytes;
+        if ((e = pool_alloc(device, (void**)&g->d_eh, bytes)) != cudaSuccess)
             return bail(cuda_fail(e, "cudaMalloc(edge hash)"));
         if ((e = cudaMemsetAsync(g->d_eh, 0xFF, bytes, g->stream)) != cudaSuccess)
             return bail(cuda_fail(e, "memset(edge hash)"));
@@ -586,12 +668,15 @@ void gmk_graph_free(gmk_graph* g) {
     if (!g) return;
     cudaSetDevice(g->device);
     if (g->stream) cudaStreamSynchronize(g->stream);
-    cudaFree(g->d_off); cudaFree(g->d_adj); cudaFree(g->d_ctr); cudaFree(g->d_order);
-    cudaFree(g->d_eh); cudaFree(g->d_rc); cudaFree(g->d_root_nodes); cudaFree(g->d_feat);
-    if (g->ev0) cudaEventDestroy(g->ev0);
-    if (g->ev1) cudaEventDestroy(g->ev1);
-    if (g->stream) cudaStreamDestroy(g->stream);
-    if (g->copy_stream) cudaStreamDestroy(g->copy_stream);
+    const int d = g->device;
+    pool_free(d, g->d_off, sizeof(uint32_t) * (g->n + 1ull));
+    pool_free(d, g->d_adj, sizeof(uint32_t) * std::max<uint64_t>(1, g->adj_len));
+    pool_free(d, g->d_ctr, sizeof(Counters));
+    pool_free(d, g->d_rc, sizeof(RoundCounters));
+    pool_free(d, g->d_eh, g->eh_bytes);
+    cudaFree(g->d_order); cudaFree(g->d_root_nodes); cudaFree(g->d_feat);
+    pool_return(d, g->stream, g->ev0);
+    pool_return(d, g->copy_stream, g->ev1);
     delete g;
 }
 
@@ -630,8 +715,8 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
     if (!di.ready) {
         int sms = 0;
         CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&di.per_sm_warp,
-                                                         enumerate_warp_kernel<false>, kWBlock, 0));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &di.per_sm_warp, enumerate_warp_kernel<false, false>, kWBlock, 0));
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&di.per_sm_thread, enumerate_kernel,
                                                          kBlock, 0));
         di.sms = sms;
@@ -657,15 +742,25 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
                                                         1ull << 30);
         }
     }
-    const uint32_t smax = opts->max_members ? opts->max_members : kDefaultSmax;
+    // Members of a k-biplex: every x misses at most k of Y, so |Y| <= (max U
+    // degree) + k, and |X| <= (max V degree) + k.  The warp engine sizes its
+    // member buffers to that bound (the thread engine keeps the default).
+    uint32_t smax = opts->max_members ? opts->max_members : kDefaultSmax;
+    if (warp && !opts->max_members) {
+        uint64_t bound = 0;
+        for (const GraphJob& j : jobs)
+            bound = std::max<uint64_t>(bound, (uint64_t)j.g->max_degree_side[0] +
+                                                  j.g->max_degree_side[1] + 2ull * j.k + 2);
+        smax = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(smax, bound), 1ull << 24);
+    }
     // workers: threads (thread engine) or warps (warp engine)
     uint64_t threads = opts->threads ? opts->threads : (uint64_t)di.sms * per_sm * block;
     threads = std::max<uint64_t>(threads, (uint64_t)block);
     // keep the search arenas within 40% of free device memory (asked only when
     // the cached workspace is too small)
-    const uint64_t per_worker = 4ull * arena_words + 8ull * smax;
+    const uint64_t per_worker = 4ull * arena_words + 12ull * smax;
     uint64_t workers = threads / lanes_per_worker;
-    if (workers * 4ull * arena_words > ws.arena_bytes || workers * 8ull * smax > ws.sbuf_bytes) {
+    if (workers * 4ull * arena_words > ws.arena_bytes || workers * 12ull * smax > ws.sbuf_bytes) {
         size_t free_b = 0, total_b = 0;
         CK(cudaMemGetInfo(&free_b, &total_b));
         const uint64_t budget = (uint64_t)((double)(free_b + ws.arena_bytes + ws.sbuf_bytes) * 0.4);
@@ -676,7 +771,7 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
     workers = threads / lanes_per_worker;
     int rc;
     if ((rc = grow((void**)&ws.d_arena, &ws.arena_bytes, workers * 4ull * arena_words))) return rc;
-    if ((rc = grow((void**)&ws.d_sbuf, &ws.sbuf_bytes, workers * 8ull * smax))) return rc;
+    if ((rc = grow((void**)&ws.d_sbuf, &ws.sbuf_bytes, workers * 12ull * smax))) return rc;
 
     // per graph: root x with chunks of its first-level children
     const size_t ng = jobs.size();
@@ -833,10 +928,12 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
             a.out_buf = opts->emit ? outb[round & 1] : nullptr;
             CK(cudaMemsetAsync(g0->d_rc, 0, sizeof(RoundCounters), g0->stream));
             CK(cudaMemsetAsync(&g0->d_rc->out_fail, 0xFF, 2 * sizeof(unsigned long long), g0->stream));
-            if (ng == 1)
-                enumerate_warp_kernel<false><<<grid, kWBlock, 0, g0->stream>>>(a);
-            else
-                enumerate_warp_kernel<true><<<grid, kWBlock, 0, g0->stream>>>(a);
+            if (ng == 1 && !opts->emit)
+                enumerate_warp_kernel<false, false><<<grid, kWBlock, 0, g0->stream>>>(a);
+            else if (ng == 1)
+                enumerate_warp_kernel<false, true><<<grid, kWBlock, 0, g0->stream>>>(a);
+            else   // a batch has no records
+                enumerate_warp_kernel<true, false><<<grid, kWBlock, 0, g0->stream>>>(a);
             CK(cudaGetLastError());
             if (pending >= 0 && sink_rc == GMK_OK) {
                 sink_rc = deliver_records(g0, outb[pending], pending_words, sink, user);

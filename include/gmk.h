@@ -85,7 +85,9 @@ typedef struct {
     uint32_t chunk;           /* first-level children per task (batched); 0 = automatic */
     uint32_t threads;         /* resident search threads; 0 = automatic */
     uint32_t arena_words;     /* per-thread search arena (u32 words); 0 = automatic */
-    uint32_t max_members;     /* largest |X|+|Y| a task may hold; 0 = 2048 */
+    uint32_t max_members;     /* largest |X|+|Y| a task may hold; 0 = the bound
+                                 (max U degree + max V degree + 2k + 2, at least 2048)
+                                 for the warp engine, 2048 for the thread engine */
     uint32_t watchdog_ms;     /* stop with GMK_E_TIMEOUT after this long; 0 = none */
     uint64_t out_words;       /* emit-mode record buffer (u32 words); 0 = automatic */
     const float* task_cost;   /* GMK_SCHEDULE_ORDERED: one cost per root U vertex (n_left) */

@@ -282,30 +282,33 @@ __global__ void __launch_bounds__(kWBlock, GMK_WARP_MIN_BLOCKS) enumerate_warp_k
     flush(t, o);
 }
 
-// CSR check on the device, one thread per vertex: offsets non-decreasing and
-// within adj, rows strictly ascending and holding ids of the other side only.
-// Also folds the CSR into an order-dependent 64-bit sum (the graph's
-// fingerprint, used to match checkpoints to graphs).
+// CSR check on the device: thread i checks vertex i (offsets non-decreasing
+// and within adj) and adjacency entry i (inside its row, ascending, an id of
+// the other side), so a hub's row is spread over many threads.  It also folds
+// the CSR into an order-dependent 64-bit sum (the graph's fingerprint, used
+// to match checkpoints to graphs).
 __global__ void csr_check_kernel(const uint32_t* off, const uint32_t* adj, uint32_t n, uint32_t nl,
                                  unsigned long long adj_len, int* bad, unsigned long long* fp) {
-    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= n) return;
-    const uint32_t a = off[v], b = off[v + 1];
-    unsigned long long h = gmk::mix64(((unsigned long long)v << 32 | a) ^ 0x6A09E667F3BCC909ull);
-    if (a > b || b > adj_len) {
-        atomicExch(bad, 1);
-        return;
+    const unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long h = 0;
+    if (i < n) {
+        const uint32_t a = off[i], b = off[i + 1];
+        if (a > b || b > adj_len) atomicExch(bad, 1);
+        h += gmk::mix64(((unsigned long long)i << 32 | a) ^ 0x6A09E667F3BCC909ull);
     }
-    const uint32_t lo = v < nl ? nl : 0u, hi = v < nl ? n : nl;
-    for (uint32_t p = a; p < b; ++p) {
-        const uint32_t w = adj[p];
-        if (w < lo || w >= hi || (p > a && adj[p - 1] >= w)) {
-            atomicExch(bad, 1);
-            return;
+    if (i < adj_len) {
+        // the row holding entry i: the last v with off[v] <= i
+        uint32_t lo = 0, hi = n;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (off[mid] <= i) lo = mid; else hi = mid;
         }
-        h += gmk::mix64(((unsigned long long)p << 32 | w) ^ 0xBB67AE8584CAA73Bull);
+        const uint32_t w = adj[i];
+        const uint32_t side_lo = lo < nl ? nl : 0u, side_hi = lo < nl ? n : nl;
+        if (w < side_lo || w >= side_hi || (i > off[lo] && adj[i - 1] >= w)) atomicExch(bad, 1);
+        h += gmk::mix64((i << 32 | w) ^ 0xBB67AE8584CAA73Bull);
     }
-    atomicAdd(fp, h);
+    if (h) atomicAdd(fp, h);
 }
 
 bool read_file(const char* path, std::vector<uint32_t>& words) {
@@ -515,9 +518,10 @@ int upload(const uint32_t* off, const uint32_t* adj, uint32_t n, uint32_t nl, in
         Check* dc = reinterpret_cast<Check*>(g->d_rc);   // scratch until the first enumeration
         if ((e = cudaMemsetAsync(dc, 0, sizeof(Check), g->stream)) != cudaSuccess)
             return bail(cuda_fail(e, "memset(check)"));
-        if (n) {
-            csr_check_kernel<<<(n + 255) / 256, 256, 0, g->stream>>>(g->d_off, g->d_adj, n, nl,
-                                                                     g->adj_len, &dc->bad, &dc->fp);
+        const unsigned long long items = std::max<unsigned long long>(n, g->adj_len);
+        if (items) {
+            csr_check_kernel<<<(unsigned)((items + 255) / 256), 256, 0, g->stream>>>(
+                g->d_off, g->d_adj, n, nl, g->adj_len, &dc->bad, &dc->fp);
             if ((e = cudaGetLastError()) != cudaSuccess) return bail(cuda_fail(e, "csr_check"));
         }
         if ((e = cudaMemcpyAsync(&hc, dc, sizeof(hc), cudaMemcpyDeviceToHost, g->stream)) != cudaSuccess ||

@@ -52,14 +52,18 @@ int gmk_graph_load(const char* path, int device, gmk_graph** out);
 int gmk_graph_from_csr(const uint32_t* offsets, const uint32_t* adj, uint32_t n,
                        uint32_t n_left, int device, gmk_graph** out);
 
-/* Sizes of a loaded graph (any pointer may be NULL). */
+/* Sizes of a loaded graph (any pointer may be NULL): the header fields the
+ * reference reads in load_graph_from_bin (data/src/tmp_load.h:213-295). */
 int gmk_graph_info(const gmk_graph* g, uint32_t* n, uint32_t* n_left, uint64_t* adj_len);
 
-/* 64-bit order-dependent hash of the graph's CSR, computed on the device at
- * load; the identity that checkpoints and tuning caches record. */
+/* No counterpart in the reference.  64-bit order-dependent hash of the graph's
+ * CSR, computed on the device at load; the identity that checkpoints and tuning
+ * caches record. */
 int gmk_graph_fingerprint(const gmk_graph* g, uint64_t* out);
 
-/* Releases device memory (the CSR and any cached enumeration workspace). */
+/* Releases the graph's device memory (its buffers go to a per-device cache for
+ * the next load).  The reference frees its device arrays when the process
+ * exits; there is no separate call. */
 void gmk_graph_free(gmk_graph* g);
 
 /* Schedules of the search tasks (one task = a root U vertex and a chunk of its
@@ -126,7 +130,9 @@ typedef struct {
 typedef int (*gmk_sink)(void* user, const uint32_t* x, uint32_t nx, const uint32_t* y,
                         uint32_t ny);
 
-/* Fills *o with the defaults (k = 1, no limit, batched schedule). */
+/* Fills *o with the defaults: k = 1 as the reference's -k (src/main.cu:1722-1732),
+ * no result limit (the gmk CLI applies the reference's -r default of 10^7), the
+ * batched schedule and the warp engine. */
 void gmk_opts_default(gmk_opts* o);
 
 /* Replaces: enumerate_GPU (reference src/main.cu:999-1580) with everything it
@@ -224,13 +230,17 @@ int gmk_mlp_train(gmk_mlp* m, const float* x, const float* y, uint32_t n, uint32
                   float lr, float* loss);
 int gmk_mlp_predict(gmk_mlp* m, const float* x, uint32_t n, float* out);
 
-/* Canonical per-result hash pair (the set summary's h1/h2): ids are the
- * global ids of X u Y in any order, nx = |X|, ny = |Y|.  Host-only. */
+/* No counterpart in the reference.  Canonical per-result hash pair (the set
+ * summary's h1/h2): ids are the global ids of X u Y in any order, nx = |X|,
+ * ny = |Y|.  Host-only. */
 void gmk_result_hash(const uint32_t* ids, uint32_t n_ids, uint32_t nx, uint32_t ny,
                      uint64_t* h1, uint64_t* h2);
 
+/* Replace CUDA_ERROR_CHECK's message-and-exit(1) (include/utils.h:42-49): the
+ * name of a GMK_E* code, and the text of the last CUDA failure on this thread. */
 const char* gmk_strerror(int code);
 const char* gmk_last_cuda_error(void);
+/* No counterpart in the reference: GMK_ABI_VERSION of the loaded library. */
 int gmk_abi_version(void);
 
 #ifdef __cplusplus

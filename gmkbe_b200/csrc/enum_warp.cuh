@@ -1065,7 +1065,10 @@ __device__ unsigned long long run_dfs(Ctx& t, const Outputs& o, uint32_t first,
     bool may_split = sb != nullptr && (lim.split_min_nodes != 0 || lim.drain_at != 0);
     while (cur != kNoPos) {
         if (t.err) break;
-        if ((++polls & 15u) == 0) {
+#ifndef GMK_POLL_MASK
+#define GMK_POLL_MASK 15u    // stop / watchdog / split checks every 16 loop steps
+#endif
+        if ((++polls & GMK_POLL_MASK) == 0) {
             int stop = 0, late = 0, hungry = 0;
             if (t.lane == 0) {
                 stop = load_flag(o.stop);

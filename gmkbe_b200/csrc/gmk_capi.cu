@@ -62,7 +62,11 @@ struct RoundCounters {
 constexpr int kBlock = 128;
 constexpr uint32_t kDefaultArena = 1u << 16;
 constexpr uint32_t kDefaultSmax = 2048;
-constexpr uint32_t kDefaultPairLimit = 4096;
+// Node rules run while |S u C_U| x |S u C_V| is at most this (gmk_opts.pair_limit 0).
+#ifndef GMK_PAIR_LIMIT
+#define GMK_PAIR_LIMIT 4096
+#endif
+constexpr uint32_t kDefaultPairLimit = GMK_PAIR_LIMIT;
 
 __global__ void __launch_bounds__(kBlock)
 enumerate_kernel(gmk::GraphView g, uint32_t k, Counters* ctr, uint32_t* arenas,
@@ -103,13 +107,16 @@ enumerate_kernel(gmk::GraphView g, uint32_t k, Counters* ctr, uint32_t* arenas,
     gmk::flush(t, o);
 }
 
-constexpr int kWBlock = 128;                 // 4 warps per block
+#ifndef GMK_WARP_BLOCK
+#define GMK_WARP_BLOCK 128                   // threads per block of the warp engine
+#endif
+constexpr int kWBlock = GMK_WARP_BLOCK;
 constexpr int kWarpsPerBlock = kWBlock / 32;
-// Resident blocks per SM the register allocation targets.  5 blocks (20 warps
-// per SM) leaves 96 registers a thread and no spills; measured faster on B200
-// than 32 warps per SM at 64 registers with spills.
+// Resident blocks per SM the register allocation targets.  6 blocks (24 warps
+// per SM, 80 registers a thread, a few spills) measured 6 % faster on B200 than
+// 5 blocks at 96 registers without spills, and 20 % faster than 4.
 #ifndef GMK_WARP_MIN_BLOCKS
-#define GMK_WARP_MIN_BLOCKS 5
+#define GMK_WARP_MIN_BLOCKS 6
 #endif
 constexpr uint32_t kDefaultWarpArena = 1u << 18;
 

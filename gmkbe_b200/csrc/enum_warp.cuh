@@ -397,6 +397,59 @@ __device__ bool outsider_addable(Ctx& t, const uint32_t* l0, uint32_t n0, const 
     }
     bk0 = warp_min64(bk0);
     bk1 = warp_min64(bk1);
+    if (bk0 != ~0ull && bk1 != ~0ull) {
+        // Both sides have a blocker (the usual case): an outsider of side s
+        // must be adjacent to side o's blocker, so each side scans one row.
+        // Both rows go through one pass of lane groups (side-0 entries first),
+        // so that their dependent loads overlap; the answer is the same "or".
+        const uint32_t b1 = (uint32_t)bk1, b0 = (uint32_t)bk0;
+        const uint32_t m0 = b1 < t.ns ? t.sid[b1] : l1[2 * (b1 - t.ns)];   // rows of side-0 outsiders
+        const uint32_t m1 = b0 < t.ns ? t.sid[b0] : l0[2 * (b0 - t.ns)];   // rows of side-1 outsiders
+        const uint32_t d0 = degree(g, m0), d = d0 + degree(g, m1);
+        const uint32_t* r0 = g.adj + g.off[m0];
+        const uint32_t* r1 = g.adj + g.off[m1];
+        if (t.lane == 0) t.work += d;
+        const Groups gr = make_groups(d, t.ns + (n0 > n1 ? n0 : n1), t.lane);
+        #pragma unroll 1
+        for (uint32_t base = 0; base < d; base += gr.rows) {
+            const uint32_t p = base + gr.row;
+            const bool live = p < d;
+            const int s = p >= d0;                     // the outsider's side
+            const uint32_t e = live ? (s ? r1[p - d0] : r0[p]) : 0u;
+            const uint32_t* ls = s ? l1 : l0;
+            const uint32_t* lo = s ? l0 : l1;
+            const uint32_t cs = s ? n1 : n0, co = s ? n0 : n1;
+            const uint32_t* tots_o = tot + t.ns + (s ? 0u : n0);
+            // skipped: in S or in C_s
+            bool skip = false;
+            if (live) {
+                #pragma unroll 1
+                for (uint32_t j = gr.slot; j < t.ns + cs && !skip; j += gr.G)
+                    skip = j < t.ns ? t.sid[j] == e : ls[2 * (j - t.ns)] == e;
+            }
+            skip = group_any(skip, gr);
+            // misses against S_o u C_o: at most k, none on a member already at k
+            bool bad = !live || skip;
+            uint32_t miss = 0;
+            if (!bad) {
+                #pragma unroll 1
+                for (uint32_t j = gr.slot; j < t.ns + co && !bad; j += gr.G) {
+                    if (j < t.ns) {
+                        const uint32_t w = t.sid[j];
+                        if (side_of(g, w) == s || adj_test(t, e, w)) continue;
+                        bad = ++miss > t.k || tot[j] >= t.k;
+                    } else {
+                        if (adj_test(t, e, lo[2 * (j - t.ns)])) continue;
+                        bad = ++miss > t.k || tots_o[j - t.ns] >= t.k;
+                    }
+                }
+            }
+            bad = group_any(bad, gr);
+            miss = group_sum(miss, gr);
+            if (__any_sync(kFull, !bad && miss <= t.k)) return true;
+        }
+        return false;
+    }
     #pragma unroll 1
     for (int s = 0; s < 2; ++s) {
         const int o = 1 - s;

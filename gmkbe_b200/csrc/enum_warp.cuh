@@ -39,6 +39,10 @@ namespace warp {
 constexpr unsigned kFull = 0xFFFFFFFFu;
 constexpr uint32_t kSrcCap = 17;          // k + 1 sources, k <= 16
 constexpr uint32_t FL_ROOT = 16u;         // frame flag: the task's root frame
+constexpr uint32_t FL_BITS0 = 32u;        // frame flags: filter bitmaps of list 0 / list 1
+constexpr uint32_t FL_BITS1 = 64u;        //   follow the frame's lists (add_filter_bits)
+constexpr uint32_t kBitsMinList = 64;     // shorter lists filter their children by probing
+constexpr uint32_t kBitsMaxZ = 8;         // bitmaps for at most this many members
 constexpr unsigned long long kEmptyKey = ~0ull;
 
 // Open-addressing set of edges, keys (u << 32 | v) with u in U, v in V, in
@@ -764,7 +768,78 @@ __device__ __forceinline__ void append_pair(Ctx& t, uint32_t w, uint32_t& cnt, b
     cnt += __popc(mask);
 }
 
+// Filter bitmaps.  When a child S + c of a frame is built, the members of the
+// other side that c brings to k misses (sat(c)) must be adjacent to every
+// candidate kept on c's side.  sat(c) lies in Z, the other side's members at
+// k - 1 misses in the frame.  For a long list that adjacency test repeats for
+// every child (O(n^2) probes per frame), so a frame that branches on a list
+// of kBitsMinList or more entries gets one bitmap per member of Z (up to
+// kBitsMaxZ): bit q = list entry q is adjacent to z.  Layout, right after the
+// frame's lists (list 0's region first when both exist):
+//   [nz, z_0 .. z_nz-1, bitmap of z_0 (ceil(n / 32) words), ..., bitmap of z_nz-1]
+// Split records do not carry them; a restored frame filters by probing.
+__device__ __forceinline__ uint32_t bits_region(const Ctx& t, uint32_t cur, const Hdr& f, int s) {
+    uint32_t at = cur + F_WORDS + 2 * (((f.flags & FL_G0) ? 0u : f.cnt.a) + ((f.flags & FL_G1) ? 0u : f.cnt.b));
+    if (s == 1 && (f.flags & FL_BITS0)) {
+        const uint32_t nz0 = t.arena[at];
+        at += 1 + nz0 + nz0 * ((f.cnt.a + 31) >> 5);
+    }
+    return at;
+}
+
+// Builds the bitmaps of frame cur (called when it starts branching).
+__device__ __forceinline__ void add_filter_bits(Ctx& t, uint32_t cur, const Hdr& f) {
+    uint32_t top = f.top, flags = 0;
+    #pragma unroll 1
+    for (int s = 0; s < 2; ++s) {
+        const uint32_t n = f.cnt.get(s);
+        if ((f.flags & gbit(s)) || n < kBitsMinList) continue;
+        const int o = 1 - s;
+        // Z: members of side o at k - 1 misses, in S order
+        uint32_t nz = 0;
+        #pragma unroll 1
+        for (uint32_t base = 0; base < t.ns; base += 32) {
+            const uint32_t i = base + t.lane;
+            const bool on = i < t.ns && side_of(t.g, t.sid[i]) == o && t.smc[i] + 1 == t.k;
+            const uint32_t mask = __ballot_sync(kFull, on);
+            if (on) {
+                const uint32_t r = nz + __popc(mask & lanemask_lt());
+                if (r < kBitsMaxZ && top + 1 + r < t.cap) t.arena[top + 1 + r] = t.sid[i];
+            }
+            nz += __popc(mask);
+        }
+        const uint32_t nw = (n + 31) >> 5;
+        if (nz == 0 || nz > kBitsMaxZ) continue;
+        if (top + 1ull + nz + (unsigned long long)nz * nw > t.cap) break;   // no room: children probe
+        if (t.lane == 0) t.arena[top] = nz;
+        __syncwarp();
+        const uint32_t* lst = t.arena + f.off.get(s);
+        uint32_t* bm = t.arena + top + 1 + nz;
+        #pragma unroll 1
+        for (uint32_t j = 0; j < nz; ++j) {
+            const uint32_t z = t.arena[top + 1 + j];
+            #pragma unroll 1
+            for (uint32_t base = 0; base < n; base += 32) {
+                const uint32_t q = base + t.lane;
+                const bool a = q < n && adj_test(t, lst[2 * q], z);
+                const uint32_t word = __ballot_sync(kFull, a);
+                if (t.lane == 0) bm[j * nw + (base >> 5)] = word;
+            }
+        }
+        flags |= s ? FL_BITS1 : FL_BITS0;
+        top += 1 + nz + nz * nw;
+    }
+    if (flags) {
+        if (t.lane == 0) {
+            t.arena[cur + F_FLAGS] |= flags;
+            t.arena[cur + F_TOP] = top;
+        }
+        __syncwarp();
+    }
+}
+
 // Warp form of build_child (enum_core.cuh): the child "S + c" of frame cur.
+template <bool kBits>
 __device__ uint32_t build_child(Ctx& t, const Outputs& o, uint32_t cur, uint32_t c, int s,
                                 uint32_t p, bool forced, bool opp_done) {
     const GraphView& g = t.g;
@@ -817,6 +892,23 @@ __device__ uint32_t build_child(Ctx& t, const Outputs& o, uint32_t cur, uint32_t
         const uint32_t n = f.cnt.get(s);
         if (w + 2ull * n > t.cap) { fail(t, o, TASK_E_ARENA); return kNoPos; }
         const uint32_t start = forced ? 0u : p + 1;
+        // the frame's filter bitmaps, when it has them: sel = the rows of sat(c)
+        const uint32_t* bm = nullptr;
+        uint32_t sel = 0, nw = 0;
+        if (kBits && nsat && (f.flags & (s ? FL_BITS1 : FL_BITS0))) {
+            const uint32_t* reg = t.arena + bits_region(t, cur, f, s);
+            const uint32_t nz = reg[0];
+            bool all = true;
+            #pragma unroll 1
+            for (uint32_t i = 0; i < nsat && all; ++i) {
+                uint32_t j = 0;
+                #pragma unroll 1
+                while (j < nz && reg[1 + j] != t.sat[i]) ++j;
+                all = j < nz;
+                sel |= all ? 1u << j : 0u;
+            }
+            if (all) { bm = reg + 1 + nz; nw = (n + 31) >> 5; }
+        }
         #pragma unroll 1
         for (uint32_t base = start; base < n; base += 32) {
             const uint32_t q = base + t.lane;
@@ -826,8 +918,14 @@ __device__ uint32_t build_child(Ctx& t, const Outputs& o, uint32_t cur, uint32_t
                 v = lst[2 * q];
                 m = lst[2 * q + 1];
                 keep = true;
-                #pragma unroll 1
-                for (uint32_t i = 0; i < nsat && keep; ++i) keep = adj_test(t, v, t.sat[i]);
+                if (kBits && bm) {
+                    #pragma unroll 1
+                    for (uint32_t r = sel; r && keep; r &= r - 1)
+                        keep = (bm[(__ffs(r) - 1) * nw + (q >> 5)] >> (q & 31)) & 1u;
+                } else {
+                    #pragma unroll 1
+                    for (uint32_t i = 0; i < nsat && keep; ++i) keep = adj_test(t, v, t.sat[i]);
+                }
             }
             append_pair(t, w, cnt, keep, v, m);
         }
@@ -931,7 +1029,7 @@ struct ChildReq {
 
 // Warp form of enter_node (enum_core.cuh).  ENTER_PUSHED: a forced candidate
 // was found; *req describes the child to build.
-template <bool kRec>
+template <bool kRec, bool kBits>
 __device__ int enter_node(Ctx& t, const Outputs& o, uint32_t cur, ChildReq* req) {
     const GraphView& g = t.g;
     const Hdr f = read_hdr(t.arena + cur);
@@ -1078,6 +1176,8 @@ __device__ int enter_node(Ctx& t, const Outputs& o, uint32_t cur, ChildReq* req)
         fw[F_POS] = (f.flags & gbit((int)order)) ? f.lo.get(order) + 1 : 0;
     }
     __syncwarp();
+    if (kBits && ((!g0 && f.cnt.a >= kBitsMinList) || (!g1 && f.cnt.b >= kBitsMinList)))
+        add_filter_bits(t, cur, f);
     return ENTER_ITERATE;
 }
 
@@ -1262,9 +1362,9 @@ __device__ __forceinline__ bool draining(const RunLimits& lim) {
 
 // Depth-first search from the frame at arena offset 0; returns the nodes it
 // entered.
-template <bool kRec>
-__device__ unsigned long long run_dfs(Ctx& t, const Outputs& o, uint32_t first,
-                                      const SplitBuf* sb, const RunLimits& lim) {
+template <bool kRec, bool kBits>
+__device__ __forceinline__ unsigned long long run_dfs(Ctx& t, const Outputs& o, uint32_t first,
+                                                     const SplitBuf* sb, const RunLimits& lim) {
     uint32_t cur = 0;
     uint32_t polls = 0;
     unsigned long long task_nodes = 0;
@@ -1301,7 +1401,7 @@ __device__ unsigned long long run_dfs(Ctx& t, const Outputs& o, uint32_t first,
             __syncwarp();
             t.nodes++;
             task_nodes++;
-            const int r = enter_node<kRec>(t, o, cur, &req);
+            const int r = enter_node<kRec, kBits>(t, o, cur, &req);
             if (kRec && r == ENTER_DEFER) {
                 // re-enter this node next round, after the host drained the buffer
                 set_word(t, cur + F_FLAGS, flags);
@@ -1322,7 +1422,7 @@ __device__ unsigned long long run_dfs(Ctx& t, const Outputs& o, uint32_t first,
         }
         if (!want) want = next_child(t, cur, &req);
         if (!want) { cur = f[F_PARENT_SLOT]; continue; }
-        const uint32_t ch = build_child(t, o, cur, req.c, req.s, req.p, req.forced, req.opp_done);
+        const uint32_t ch = build_child<kBits>(t, o, cur, req.c, req.s, req.p, req.forced, req.opp_done);
         cur = ch == kNoPos ? f[F_PARENT_SLOT] : ch;   // kNoPos: t.err is set, the loop ends
     }
     pop_to(t, 0);
@@ -1330,7 +1430,7 @@ __device__ unsigned long long run_dfs(Ctx& t, const Outputs& o, uint32_t first,
 }
 
 // Root task: x in U with its first-level children y in [first, last).
-template <bool kRec>
+template <bool kRec, bool kBits>
 __device__ unsigned long long run_root(Ctx& t, const Outputs& o, uint32_t root, uint32_t first,
                                        uint32_t last, const SplitBuf* sb, const RunLimits& lim) {
     t.ns = 0; t.nss.a = t.nss.b = 0;
@@ -1351,11 +1451,11 @@ __device__ unsigned long long run_root(Ctx& t, const Outputs& o, uint32_t root, 
         }
     if (t.lane == 0) write_hdr(t.arena, h);
     __syncwarp();
-    return run_dfs<kRec>(t, o, first, sb, lim);
+    return run_dfs<kRec, kBits>(t, o, first, sb, lim);
 }
 
 // Resumed task: a frame written by split_path (its S starts with the root).
-template <bool kRec>
+template <bool kRec, bool kBits>
 __device__ unsigned long long run_record(Ctx& t, const Outputs& o, const uint32_t* r,
                                          const SplitBuf* sb, const RunLimits& lim) {
     const uint32_t ns = r[0], c0 = r[1], c1 = r[2];
@@ -1379,6 +1479,7 @@ __device__ unsigned long long run_record(Ctx& t, const Outputs& o, const uint32_
     t.mask_base = ns;
     const uint32_t* fr = rs + 2 * ns;
     Hdr h = read_hdr(fr);
+    h.flags &= ~(FL_BITS0 | FL_BITS1);   // bitmaps are not part of a record
     h.off.a = F_WORDS;
     h.off.b = F_WORDS + 2 * c0;
     h.top = F_WORDS + 2 * (c0 + c1);
@@ -1388,7 +1489,7 @@ __device__ unsigned long long run_record(Ctx& t, const Outputs& o, const uint32_
     for (uint32_t i = t.lane; i < 2 * (c0 + c1); i += 32) t.arena[F_WORDS + i] = lr[i];
     if (t.lane == 0) write_hdr(t.arena, h);
     __syncwarp();
-    return run_dfs<kRec>(t, o, 0, sb, lim);
+    return run_dfs<kRec, kBits>(t, o, 0, sb, lim);
 }
 
 }  // namespace warp

@@ -181,7 +181,7 @@ __device__ __forceinline__ const GraphTask& use_graph(const WarpArgs& a, uint32_
 
 // kBatch: several graphs per launch; kRec: results written as records (the
 // count-only instantiation carries none of the record and drain code).
-template <bool kBatch, bool kRec>
+template <bool kBatch, bool kRec, bool kBits>
 __global__ void __launch_bounds__(kWBlock, GMK_WARP_MIN_BLOCKS) enumerate_warp_kernel(const WarpArgs a) {
     __shared__ uint32_t s_sat[kWarpsPerBlock][gmk::kSatCap];
     __shared__ uint32_t s_src[kWarpsPerBlock][gmk::warp::kSrcCap];
@@ -271,14 +271,14 @@ __global__ void __launch_bounds__(kWBlock, GMK_WARP_MIN_BLOCKS) enumerate_warp_k
             const uint32_t first = t.g.nl + c * G.chunk;
             const unsigned long long end = (unsigned long long)first + G.chunk;
             const uint32_t last = end < t.g.n ? (uint32_t)end : t.g.n;
-            const unsigned long long nodes = run_root<kRec>(t, o, root, first, last, sb, lim);
+            const unsigned long long nodes = run_root<kRec, kBits>(t, o, root, first, last, sb, lim);
             if (G.root_nodes && lane == 0) atomicAdd(G.root_nodes + root, nodes);
         } else {
             const uint32_t* rec = a.cur_words + a.cur_idx[j];
             const GraphTask& G = use_graph<kBatch>(a, kBatch ? rec[3] : 0u, t, o);
             // a round that winds down hands its queued records on unchanged
             if (!(kRec && sb && draining(lim) && forward_record(t, *sb, rec))) {
-                const unsigned long long nodes = run_record<kRec>(t, o, rec, sb, lim);
+                const unsigned long long nodes = run_record<kRec, kBits>(t, o, rec, sb, lim);
                 if (G.root_nodes && lane == 0)
                     atomicAdd(G.root_nodes + rec[gmk::warp::kRecHeader], nodes);
             }
@@ -730,7 +730,7 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
         int sms = 0;
         CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &di.per_sm_warp, enumerate_warp_kernel<false, false>, kWBlock, 0));
+            &di.per_sm_warp, enumerate_warp_kernel<false, false, false>, kWBlock, 0));
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&di.per_sm_thread, enumerate_kernel,
                                                          kBlock, 0));
         di.sms = sms;
@@ -942,12 +942,19 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
             a.out_buf = opts->emit ? outb[round & 1] : nullptr;
             CK(cudaMemsetAsync(g0->d_rc, 0, sizeof(RoundCounters), g0->stream));
             CK(cudaMemsetAsync(&g0->d_rc->out_fail, 0xFF, 2 * sizeof(unsigned long long), g0->stream));
-            if (ng == 1 && !opts->emit)
-                enumerate_warp_kernel<false, false><<<grid, kWBlock, 0, g0->stream>>>(a);
+            // k >= 2: the instantiation with filter bitmaps for long lists
+            // (at k = 1 their code alone cost 15 %, so it is a separate kernel)
+            const bool bits = a.single.k >= 2;
+            if (ng == 1 && !opts->emit && !bits)
+                enumerate_warp_kernel<false, false, false><<<grid, kWBlock, 0, g0->stream>>>(a);
+            else if (ng == 1 && !opts->emit)
+                enumerate_warp_kernel<false, false, true><<<grid, kWBlock, 0, g0->stream>>>(a);
+            else if (ng == 1 && !bits)
+                enumerate_warp_kernel<false, true, false><<<grid, kWBlock, 0, g0->stream>>>(a);
             else if (ng == 1)
-                enumerate_warp_kernel<false, true><<<grid, kWBlock, 0, g0->stream>>>(a);
+                enumerate_warp_kernel<false, true, true><<<grid, kWBlock, 0, g0->stream>>>(a);
             else   // a batch has no records
-                enumerate_warp_kernel<true, false><<<grid, kWBlock, 0, g0->stream>>>(a);
+                enumerate_warp_kernel<true, false, false><<<grid, kWBlock, 0, g0->stream>>>(a);
             CK(cudaGetLastError());
             if (pending >= 0 && sink_rc == GMK_OK) {
                 sink_rc = deliver_records(g0, outb[pending], pending_words, sink, user);

@@ -187,6 +187,23 @@ def chung_lu(nu: int, nv: int, m: int, gamma: float, seed: int,
     return relabel(u, v)
 
 
+def hubs_and_sparse(n_hubs: int, n_sparse: int, n: int, d_sparse: int, seed: int) -> Graph:
+    """n_hubs V vertices adjacent to all n U vertices, plus n_sparse V vertices
+    of d_sparse random U neighbours each.  Once S holds k + 1 hubs, a node's
+    U candidates are a local list of about n entries (the union of the hubs'
+    rows), and a sparse member one miss short of k makes every child that
+    misses it filter that list: the long-list filter with few results."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    left, right = [], []
+    for h in range(n_hubs):
+        left.append(np.arange(n, dtype=np.int64))
+        right.append(np.full(n, h, dtype=np.int64))
+    for y in range(n_hubs, n_hubs + n_sparse):
+        left.append(rng.choice(n, size=d_sparse, replace=False).astype(np.int64))
+        right.append(np.full(d_sparse, y, dtype=np.int64))
+    return relabel(np.concatenate(left), np.concatenate(right))
+
+
 def induced_prefix(g: Graph, nu: int, nv: int) -> Graph:
     """Subgraph induced by the first nu U ids and first nv V ids, re-run through
     the converter ordering (isolated vertices dropped)."""

@@ -145,6 +145,27 @@ def test_chung_lu_small_against_oracle():
         assert dg.enumerate(k=1).summary() == want
 
 
+HUB_CASES = [(3, 6, 72, 4, 2, 1), (4, 8, 80, 4, 2, 2), (4, 4, 66, 4, 3, 5), (4, 5, 70, 5, 3, 3)]
+
+
+@pytest.mark.parametrize("n_hubs,n_sparse,n,d,k,seed", HUB_CASES)
+def test_long_list_filter_bitmaps_against_oracle(n_hubs, n_sparse, n, d, k, seed):
+    # k >= 2 nodes that branch on a list of 64 or more candidates filter their
+    # children through per-frame bitmaps; with k + 1 hubs in S the U list holds
+    # all n U vertices.  Count mode, split records (restored frames carry no
+    # bitmaps) and streamed records must all give the oracle's set.
+    g = gg.hubs_and_sparse(n_hubs, n_sparse, n, d, seed)
+    want = O.enumerate_oracle(g, k).summary()
+    with G.Graph.from_graph(g) as dg:
+        assert dg.enumerate(k=k).summary() == want
+        assert dg.enumerate(k=k, chunk=4, split_min_nodes=3).summary() == want
+        if k == 2:   # the k = 3 cases hold 0.5-1 M sets: count mode only
+            sets = []
+            st = dg.enumerate(k=k, sink=lambda x, y: sets.append((tuple(x), tuple(y))))
+            assert st.summary() == want
+            assert len(sets) == want[0] and O.set_summary(sets) == want
+
+
 # ---------------------------------------------------------------- edge cases
 
 def test_single_edge():

@@ -909,25 +909,54 @@ __device__ uint32_t build_child(Ctx& t, const Outputs& o, uint32_t cur, uint32_t
             }
             if (all) { bm = reg + 1 + nz; nw = (n + 31) >> 5; }
         }
-        #pragma unroll 1
-        for (uint32_t base = start; base < n; base += 32) {
-            const uint32_t q = base + t.lane;
-            bool keep = false;
-            uint32_t v = 0, m = 0;
-            if (q < n && q != p) {
-                v = lst[2 * q];
-                m = lst[2 * q + 1];
-                keep = true;
-                if (kBits && bm) {
+        if (kBits && bm) {
+            // The keep mask of list entries 32 wi .. 32 wi + 31 is the AND of
+            // sat(c)'s bitmap words wi.  Lane i computes word wbase + i; the
+            // warp then copies only the kept entries of the non-empty words.
+            #pragma unroll 1
+            for (uint32_t wbase = start >> 5; wbase < nw; wbase += 32) {
+                const uint32_t wi = wbase + t.lane;
+                uint32_t mask = 0;
+                if (wi < nw) {
+                    mask = ~0u;
                     #pragma unroll 1
-                    for (uint32_t r = sel; r && keep; r &= r - 1)
-                        keep = (bm[(__ffs(r) - 1) * nw + (q >> 5)] >> (q & 31)) & 1u;
-                } else {
+                    for (uint32_t r = sel; r; r &= r - 1) mask &= bm[(__ffs(r) - 1) * nw + wi];
+                    const uint32_t q0 = wi << 5;
+                    if (q0 < start) mask &= start - q0 < 32 ? ~0u << (start - q0) : 0u;
+                    if (n - q0 < 32) mask &= (1u << (n - q0)) - 1u;
+                    if (p >= q0 && p - q0 < 32) mask &= ~(1u << (p - q0));
+                }
+                uint32_t live = __ballot_sync(kFull, mask != 0);
+                #pragma unroll 1
+                while (live) {
+                    const uint32_t j = __ffs(live) - 1;
+                    live &= live - 1;
+                    const uint32_t mj = __shfl_sync(kFull, mask, j);
+                    const uint32_t q = ((wbase + j) << 5) + t.lane;
+                    if ((mj >> t.lane) & 1u) {
+                        const uint32_t r = cnt + __popc(mj & lanemask_lt());
+                        t.arena[w + 2 * r] = lst[2 * q];
+                        t.arena[w + 2 * r + 1] = lst[2 * q + 1];
+                    }
+                    cnt += __popc(mj);
+                }
+            }
+            __syncwarp();
+        } else {
+            #pragma unroll 1
+            for (uint32_t base = start; base < n; base += 32) {
+                const uint32_t q = base + t.lane;
+                bool keep = false;
+                uint32_t v = 0, m = 0;
+                if (q < n && q != p) {
+                    v = lst[2 * q];
+                    m = lst[2 * q + 1];
+                    keep = true;
                     #pragma unroll 1
                     for (uint32_t i = 0; i < nsat && keep; ++i) keep = adj_test(t, v, t.sat[i]);
                 }
+                append_pair(t, w, cnt, keep, v, m);
             }
-            append_pair(t, w, cnt, keep, v, m);
         }
     }
     ch.cnt.set(s, cnt);

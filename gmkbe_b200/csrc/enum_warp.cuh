@@ -776,13 +776,16 @@ __device__ __forceinline__ void append_pair(Ctx& t, uint32_t w, uint32_t& cnt, b
 // of kBitsMinList or more entries gets one bitmap per member of Z (up to
 // kBitsMaxZ): bit q = list entry q is adjacent to z.  Layout, right after the
 // frame's lists (list 0's region first when both exist):
-//   [nz, z_0 .. z_nz-1, bitmap of z_0 (ceil(n / 32) words), ..., bitmap of z_nz-1]
+//   [nz, z_0 .. z_nz-1, end_0 .. end_nz-1,
+//    bitmap of z_0 (ceil(n / 32) words), ..., bitmap of z_nz-1]
+// end_j = 1 + the last list position adjacent to z_j (0: none), so a child
+// whose candidates start past it keeps nothing without reading the bitmap.
 // Split records do not carry them; a restored frame filters by probing.
 __device__ __forceinline__ uint32_t bits_region(const Ctx& t, uint32_t cur, const Hdr& f, int s) {
     uint32_t at = cur + F_WORDS + 2 * (((f.flags & FL_G0) ? 0u : f.cnt.a) + ((f.flags & FL_G1) ? 0u : f.cnt.b));
     if (s == 1 && (f.flags & FL_BITS0)) {
         const uint32_t nz0 = t.arena[at];
-        at += 1 + nz0 + nz0 * ((f.cnt.a + 31) >> 5);
+        at += 1 + 2 * nz0 + nz0 * ((f.cnt.a + 31) >> 5);
     }
     return at;
 }
@@ -810,24 +813,27 @@ __device__ __forceinline__ void add_filter_bits(Ctx& t, uint32_t cur, const Hdr&
         }
         const uint32_t nw = (n + 31) >> 5;
         if (nz == 0 || nz > kBitsMaxZ) continue;
-        if (top + 1ull + nz + (unsigned long long)nz * nw > t.cap) break;   // no room: children probe
+        if (top + 1ull + 2 * nz + (unsigned long long)nz * nw > t.cap) break;   // no room: children probe
         if (t.lane == 0) t.arena[top] = nz;
         __syncwarp();
         const uint32_t* lst = t.arena + f.off.get(s);
-        uint32_t* bm = t.arena + top + 1 + nz;
+        uint32_t* bm = t.arena + top + 1 + 2 * nz;
         #pragma unroll 1
         for (uint32_t j = 0; j < nz; ++j) {
             const uint32_t z = t.arena[top + 1 + j];
+            uint32_t end = 0;
             #pragma unroll 1
             for (uint32_t base = 0; base < n; base += 32) {
                 const uint32_t q = base + t.lane;
                 const bool a = q < n && adj_test(t, lst[2 * q], z);
                 const uint32_t word = __ballot_sync(kFull, a);
+                if (word) end = base + 32 - __clz(word);
                 if (t.lane == 0) bm[j * nw + (base >> 5)] = word;
             }
+            if (t.lane == 0) t.arena[top + 1 + nz + j] = end;
         }
         flags |= s ? FL_BITS1 : FL_BITS0;
-        top += 1 + nz + nz * nw;
+        top += 1 + 2 * nz + nz * nw;
     }
     if (flags) {
         if (t.lane == 0) {
@@ -894,7 +900,7 @@ __device__ uint32_t build_child(Ctx& t, const Outputs& o, uint32_t cur, uint32_t
         const uint32_t start = forced ? 0u : p + 1;
         // the frame's filter bitmaps, when it has them: sel = the rows of sat(c)
         const uint32_t* bm = nullptr;
-        uint32_t sel = 0, nw = 0;
+        uint32_t sel = 0, nw = 0, end = n;
         if (kBits && nsat && (f.flags & (s ? FL_BITS1 : FL_BITS0))) {
             const uint32_t* reg = t.arena + bits_region(t, cur, f, s);
             const uint32_t nz = reg[0];
@@ -905,19 +911,23 @@ __device__ uint32_t build_child(Ctx& t, const Outputs& o, uint32_t cur, uint32_t
                 #pragma unroll 1
                 while (j < nz && reg[1 + j] != t.sat[i]) ++j;
                 all = j < nz;
-                sel |= all ? 1u << j : 0u;
+                if (all) {
+                    sel |= 1u << j;
+                    end = reg[1 + nz + j] < end ? reg[1 + nz + j] : end;
+                }
             }
-            if (all) { bm = reg + 1 + nz; nw = (n + 31) >> 5; }
+            if (all) { bm = reg + 1 + 2 * nz; nw = (n + 31) >> 5; }
         }
         if (kBits && bm) {
             // The keep mask of list entries 32 wi .. 32 wi + 31 is the AND of
             // sat(c)'s bitmap words wi.  Lane i computes word wbase + i; the
             // warp then copies only the kept entries of the non-empty words.
+            const uint32_t nwe = (end + 31) >> 5;   // words up to the last kept candidate
             #pragma unroll 1
-            for (uint32_t wbase = start >> 5; wbase < nw; wbase += 32) {
+            for (uint32_t wbase = start >> 5; wbase < nwe; wbase += 32) {
                 const uint32_t wi = wbase + t.lane;
                 uint32_t mask = 0;
-                if (wi < nw) {
+                if (wi < nwe) {
                     mask = ~0u;
                     #pragma unroll 1
                     for (uint32_t r = sel; r; r &= r - 1) mask &= bm[(__ffs(r) - 1) * nw + wi];

@@ -20,12 +20,12 @@ from __future__ import annotations
 
 import argparse
 import csv
-import io
 import json
 import os
 import statistics
 import subprocess
 import sys
+import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -60,7 +60,9 @@ def _traffic_per_launch(kernel: str):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks / throttle reasons sampled every 50 ms, each sample
+    time-stamped on arrival; stop() keeps the samples inside the timed window
+    (the nearest one when the window is shorter than the sampling interval)."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -68,33 +70,53 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.p = None
+        self.rows = []
+        self.thread = None
+
+    def _read(self):
+        for line in self.p.stdout:
+            r = next(csv.reader([line]), [])
+            if len(r) >= 9:
+                self.rows.append((time.perf_counter(), r))
 
     def start(self):
+        """Starts sampling and waits (up to 5 s) for the first sample, so that
+        the timed window that follows is covered."""
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                       "--format=csv,noheader,nounits", "-lms", "50"],
                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.p = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+        t_end = time.perf_counter() + 5.0
+        while not self.rows and time.perf_counter() < t_end and self.p.poll() is None:
+            time.sleep(0.01)
 
-    def stop(self):
+    def stop(self, t0: float, t1: float):
         if not self.p:
             return None
+        time.sleep(0.06)                       # one more sample after the window
         self.p.terminate()
         try:
-            out, _ = self.p.communicate(timeout=5)
+            self.p.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.p.kill()
-            out, _ = self.p.communicate()
-        rows = [r for r in csv.reader(io.StringIO(out)) if len(r) >= 9]
-        if not rows:
+        self.thread.join(timeout=5)
+        if not self.rows:
             return None
-        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
-        mx = max((float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()), default=None)
+        inside = [r for t, r in self.rows if t0 <= t <= t1]
+        if not inside:
+            mid = 0.5 * (t0 + t1)
+            inside = [min(self.rows, key=lambda tr: abs(tr[0] - mid))[1]]
+        sm = [float(r[1]) for r in inside if r[1].strip().replace(".", "").isdigit()]
+        mx = max((float(r[2]) for r in inside if r[2].strip().replace(".", "").isdigit()), default=None)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip() == "Active"})
+        reasons = sorted({names[i] for r in inside for i in range(4) if r[5 + i].strip() == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(inside)}
 
 
 def _dist():
@@ -191,6 +213,7 @@ def run_gmk(args, world, rank, local):
     barrier()
     clocks = ClockSampler(local)
     clocks.start()
+    t_clk0 = time.perf_counter()
     ms, count, algo, launches = [], 0, 0, 0
     for _ in range(args.steps):
         flush_buf.zero_()          # L2 flush, outside the timed kernel
@@ -201,7 +224,7 @@ def run_gmk(args, world, rank, local):
         algo += st.algo_bytes
         launches += st.rounds
     barrier()
-    clk = clocks.stop()
+    clk = clocks.stop(t_clk0, time.perf_counter())
     # the plain static schedule on the same GPU (one task per root, no splitting)
     plain = None
     if args.schedule != "plain" and not args.no_plain:
@@ -210,7 +233,13 @@ def run_gmk(args, world, rank, local):
         sp = dg.enumerate(**dict(kw, schedule="plain"))
         plain = {"value": sp.count / (sp.kernel_ms / 1e3), "ms": sp.kernel_ms,
                  "results": sp.count}
-    # end to end through the C ABI: host CSR -> device, enumerate, read back
+    # end to end through the C ABI: host CSR -> device, enumerate, read back.
+    # W untimed steps first, like the device arm (the first upload of a second
+    # graph fills the device buffer cache)
+    for _ in range(args.warmup):
+        with G.Graph.from_csr(off_np, adj_np, host.n, host.n_left, device=local) as g2:
+            g2.enumerate(**kw)
+    barrier()
     e2e_s, e2e_rounds = 0.0, 0
     for _ in range(args.steps):
         flush_buf.zero_()

@@ -107,16 +107,21 @@ enumerate_kernel(gmk::GraphView g, uint32_t k, Counters* ctr, uint32_t* arenas,
     gmk::flush(t, o);
 }
 
+// One warp per block: warps are independent (no block-level sharing), and
+// single-warp blocks let the register file's last partial block count.  With
+// 25 resident blocks as the target, ptxas allocates 72 registers a thread (a
+// few spills) and 28 warps fit per SM; that measured 2-5 % faster on B200 than
+// 4-warp blocks at 80 registers (24 warps).  Among 4-warp blocks, 6 per SM (80
+// registers) was 6 % faster than 5 (96 registers, no spills) and 20 % faster
+// than 4; 7 and 8 (72 / 64 registers) lost to spills.
 #ifndef GMK_WARP_BLOCK
-#define GMK_WARP_BLOCK 128                   // threads per block of the warp engine
+#define GMK_WARP_BLOCK 32                    // threads per block of the warp engine
 #endif
 constexpr int kWBlock = GMK_WARP_BLOCK;
 constexpr int kWarpsPerBlock = kWBlock / 32;
-// Resident blocks per SM the register allocation targets.  6 blocks (24 warps
-// per SM, 80 registers a thread, a few spills) measured 6 % faster on B200 than
-// 5 blocks at 96 registers without spills, and 20 % faster than 4.
+// Resident blocks per SM the register allocation targets.
 #ifndef GMK_WARP_MIN_BLOCKS
-#define GMK_WARP_MIN_BLOCKS 6
+#define GMK_WARP_MIN_BLOCKS 25
 #endif
 constexpr uint32_t kDefaultWarpArena = 1u << 18;
 

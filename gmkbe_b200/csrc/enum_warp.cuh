@@ -123,16 +123,22 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
     return m;
 }
+// Warp reductions of 64-bit values with the 32-bit redux unit (one
+// instruction per 32-bit reduction instead of five shuffle rounds).
+// Minimum: the high words first, then the low words of the lanes holding the
+// minimal high word -- the lexicographic, i.e. numeric, minimum.
 __device__ __forceinline__ unsigned long long warp_min64(unsigned long long v) {
-    for (int o = 16; o; o >>= 1) {
-        const unsigned long long w = __shfl_xor_sync(kFull, v, o);
-        v = w < v ? w : v;
-    }
-    return v;
+    const uint32_t hi = __reduce_min_sync(kFull, (uint32_t)(v >> 32));
+    const uint32_t lo = __reduce_min_sync(kFull, (uint32_t)(v >> 32) == hi ? (uint32_t)v : ~0u);
+    return ((unsigned long long)hi << 32) | lo;
 }
+// Sum modulo 2^64: three limbs of 22, 22 and 20 bits; 32 lanes' limbs sum to
+// under 2^27, so each 32-bit reduction is exact.
 __device__ __forceinline__ unsigned long long warp_sum64(unsigned long long v) {
-    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-    return v;
+    const uint32_t l0 = __reduce_add_sync(kFull, (uint32_t)(v & 0x3FFFFFu));
+    const uint32_t l1 = __reduce_add_sync(kFull, (uint32_t)((v >> 22) & 0x3FFFFFu));
+    const uint32_t l2 = __reduce_add_sync(kFull, (uint32_t)(v >> 44));
+    return (unsigned long long)l0 + ((unsigned long long)l1 << 22) + ((unsigned long long)l2 << 44);
 }
 template <class T>
 __device__ __forceinline__ T bcast(T v) { return __shfl_sync(kFull, v, 0); }

@@ -31,6 +31,15 @@ def test_oracle_equals_definition_on_tiny_graphs(k):
     assert checked >= 30
 
 
+@pytest.mark.parametrize("args,k", [((2, 3, 8, 2, 1), 2), ((3, 3, 9, 2, 2), 2),
+                                    ((3, 2, 8, 3, 3), 3)])
+def test_oracle_equals_definition_on_hub_graphs(args, k):
+    # small members of the family the GPU filter-bitmap tests compare against
+    g = gg.hubs_and_sparse(*args)
+    assert g.n <= 15
+    assert sorted(O.enumerate_oracle(g, k, collect=True).results) == sorted(O.brute_force(g, k))
+
+
 def test_every_oracle_result_is_maximal():
     g = gg.read_graph_bin(golden_graph_path("southernwomen"))
     for k in (1, 2):

@@ -1328,6 +1328,11 @@ namespace {
 // member buffers.  Host code must not use the symbol's host-side shadow as a
 // device address; noalloc_scratch() returns the real address per device.
 static __device__ __align__(256) unsigned char g_static_scratch[GMK_STATIC_SCRATCH_BYTES];
+// Head of the scratch: the counters at 0, the CSR check's words at 128; the
+// arenas start at 256.
+constexpr uint64_t kNoallocHead = 256;
+constexpr uint64_t kNoallocCheck = 128;
+static_assert(sizeof(Counters) <= kNoallocCheck, "counters overlap the check words");
 
 std::mutex g_static_mu;
 void* g_static_addr[kMaxDevices] = {};
@@ -1354,12 +1359,14 @@ int gmk_enumerate_noalloc(const uint32_t* d_offsets, const uint32_t* d_adj, uint
     if (!d_offsets || !out || (!d_adj && n > 0) || n_left > n) return GMK_E_INVAL;
     if (k < 1 || k > 15) return GMK_E_INVAL;
     std::memset(out, 0, sizeof(*out));
-    threads = threads ? threads : 2048u;
-    threads = (threads + kBlock - 1) / kBlock * kBlock;
+    // sizes in 64 bits: a thread count near 2^32 must not wrap to a small one
+    uint64_t nthreads = threads ? threads : 2048u;
+    nthreads = (nthreads + kBlock - 1) / kBlock * kBlock;
     arena_words = arena_words ? arena_words : 4096u;
     max_members = max_members ? max_members : 512u;
-    const uint64_t need = 256ull + (uint64_t)threads * (4ull * arena_words + 8ull * max_members);
+    const uint64_t need = kNoallocHead + nthreads * (4ull * arena_words + 8ull * max_members);
     if (need > GMK_STATIC_SCRATCH_BYTES) return GMK_E_SCRATCH;
+    threads = (uint32_t)nthreads;
     int device = 0;
     CK(cudaGetDevice(&device));
     if (device < 0 || device >= kMaxDevices) return GMK_E_INVAL;
@@ -1367,8 +1374,37 @@ int gmk_enumerate_noalloc(const uint32_t* d_offsets, const uint32_t* d_adj, uint
     unsigned char* base = nullptr;
     if (int rc = noalloc_scratch(device, &base)) return rc;
     Counters* ctr = reinterpret_cast<Counters*>(base);
-    uint32_t* arenas = reinterpret_cast<uint32_t*>(base + 256);
+    uint32_t* arenas = reinterpret_cast<uint32_t*>(base + kNoallocHead);
     uint32_t* sbuf = arenas + (uint64_t)threads * arena_words;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const auto t0 = std::chrono::steady_clock::now();
+    // The caller's CSR is checked on the device before the search reads it as
+    // a graph (as gmk_graph_from_csr does): offsets non-decreasing from 0 and
+    // within adj, rows ascending, every id on the other side.  The two ends of
+    // the offsets come back through plain copies; the check's flag and
+    // fingerprint words live in the scratch's head, after the counters.
+    {
+        uint32_t ends[2] = {1u, 0u};
+        CK(cudaMemcpyAsync(&ends[0], d_offsets, 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(&ends[1], d_offsets + n, 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (ends[0] != 0) return GMK_E_FORMAT;
+        const unsigned long long adj_len = ends[1];
+        if (adj_len && !d_adj) return GMK_E_INVAL;
+        struct Check { int bad; int pad; unsigned long long fp; };
+        Check* dc = reinterpret_cast<Check*>(base + kNoallocCheck);
+        CK(cudaMemsetAsync(dc, 0, sizeof(Check), s));
+        const unsigned long long items = std::max<unsigned long long>(n, adj_len);
+        if (items) {
+            csr_check_kernel<<<(unsigned)((items + 255) / 256), 256, 0, s>>>(
+                d_offsets, d_adj, n, n_left, adj_len, &dc->bad, &dc->fp);
+            CK(cudaGetLastError());
+        }
+        int bad = 0;
+        CK(cudaMemcpyAsync(&bad, &dc->bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (bad) return GMK_E_FORMAT;
+    }
     // tasks: root x with chunks of its first-level children, about 8 per thread
     const uint32_t nv = n - n_left;
     const uint64_t per_root = (8ull * threads + n_left - 1) / n_left;
@@ -1376,8 +1412,6 @@ int gmk_enumerate_noalloc(const uint32_t* d_offsets, const uint32_t* d_adj, uint
     chunk = std::min(chunk, nv);
     const uint32_t chunks_per_root = (nv + chunk - 1) / chunk;
     const unsigned long long n_tasks = (unsigned long long)n_left * chunks_per_root;
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const auto t0 = std::chrono::steady_clock::now();
     CK(cudaMemsetAsync(ctr, 0, sizeof(Counters), s));
     gmk::GraphView gv{d_offsets, d_adj, n, n_left};
     enumerate_kernel<<<threads / kBlock, kBlock, 0, s>>>(
@@ -1410,9 +1444,14 @@ int gmk_enumerate_noalloc(const uint32_t* d_offsets, const uint32_t* d_adj, uint
 
 namespace {
 
+// Text checkpoint, format 2: besides the graph, k, schedule and root order it
+// records the shard and the result limit, so that a checkpoint is resumed only
+// by a run over the same task set.
 struct Checkpoint {
     uint64_t fingerprint = 0;
     uint32_t k = 0, schedule = 0, next_root = 0, done = 0;
+    uint32_t shard = 0, nshards = 1;
+    uint64_t limit = 0;
     uint64_t order_hash = 0, count = 0, hash_sum = 0, hash_xor = 0, nodes = 0;
 };
 
@@ -1420,16 +1459,18 @@ bool read_checkpoint(const char* path, Checkpoint& c, bool& exists) {
     FILE* fp = std::fopen(path, "r");
     exists = fp != nullptr;
     if (!fp) return false;
-    unsigned long long fpv = 0, oh = 0, cnt = 0, hs = 0, hx = 0, nd = 0;
-    unsigned k = 0, sch = 0, nr = 0, dn = 0;
+    unsigned long long fpv = 0, oh = 0, cnt = 0, hs = 0, hx = 0, nd = 0, lim = 0;
+    unsigned k = 0, sch = 0, nr = 0, dn = 0, sh = 0, nsh = 0;
     const int got = std::fscanf(fp,
-                                "gmk-checkpoint 1\ngraph %llx\nk %u\nschedule %u\norder %llx\n"
+                                "gmk-checkpoint 2\ngraph %llx\nk %u\nschedule %u\norder %llx\n"
+                                "shard %u\nnshards %u\nresult_limit %llu\n"
                                 "next_root %u\ncount %llu\nhash_sum %llx\nhash_xor %llx\n"
                                 "nodes %llu\ndone %u\n",
-                                &fpv, &k, &sch, &oh, &nr, &cnt, &hs, &hx, &nd, &dn);
+                                &fpv, &k, &sch, &oh, &sh, &nsh, &lim, &nr, &cnt, &hs, &hx, &nd, &dn);
     std::fclose(fp);
-    if (got != 10) return false;
+    if (got != 13) return false;
     c.fingerprint = fpv; c.k = k; c.schedule = sch; c.order_hash = oh; c.next_root = nr;
+    c.shard = sh; c.nshards = nsh; c.limit = lim;
     c.count = cnt; c.hash_sum = hs; c.hash_xor = hx; c.nodes = nd; c.done = dn;
     return true;
 }
@@ -1439,11 +1480,13 @@ bool write_checkpoint(const char* path, const Checkpoint& c) {
     FILE* fp = std::fopen(tmp.c_str(), "w");
     if (!fp) return false;
     std::fprintf(fp,
-                 "gmk-checkpoint 1\ngraph %016llx\nk %u\nschedule %u\norder %016llx\n"
+                 "gmk-checkpoint 2\ngraph %016llx\nk %u\nschedule %u\norder %016llx\n"
+                 "shard %u\nnshards %u\nresult_limit %llu\n"
                  "next_root %u\ncount %llu\nhash_sum %016llx\nhash_xor %016llx\nnodes %llu\n"
                  "done %u\n",
                  (unsigned long long)c.fingerprint, c.k, c.schedule,
-                 (unsigned long long)c.order_hash, c.next_root, (unsigned long long)c.count,
+                 (unsigned long long)c.order_hash, c.shard, c.nshards,
+                 (unsigned long long)c.limit, c.next_root, (unsigned long long)c.count,
                  (unsigned long long)c.hash_sum, (unsigned long long)c.hash_xor,
                  (unsigned long long)c.nodes, c.done);
     const bool ok = std::fflush(fp) == 0;
@@ -1472,9 +1515,12 @@ int gmk_enumerate_resumable(gmk_graph* g, const gmk_opts* opts, const char* chec
     Checkpoint c;
     bool exists = false;
     const uint64_t oh = order_hash(g, opts);
+    const uint32_t nsh = opts->nshards > 1 ? opts->nshards : 1u;
+    const uint32_t sh = nsh > 1 ? opts->shard : 0u;
     if (read_checkpoint(checkpoint_path, c, exists)) {
         if (c.fingerprint != g->fingerprint || c.k != opts->k ||
-            c.schedule != (uint32_t)opts->schedule || c.order_hash != oh || c.next_root > g->nl)
+            c.schedule != (uint32_t)opts->schedule || c.order_hash != oh || c.next_root > g->nl ||
+            c.shard != sh || c.nshards != nsh || c.limit != opts->result_limit)
             return GMK_E_CHECKPOINT;
     } else if (exists) {
         return GMK_E_CHECKPOINT;
@@ -1483,6 +1529,9 @@ int gmk_enumerate_resumable(gmk_graph* g, const gmk_opts* opts, const char* chec
         c.k = opts->k;
         c.schedule = (uint32_t)opts->schedule;
         c.order_hash = oh;
+        c.shard = sh;
+        c.nshards = nsh;
+        c.limit = opts->result_limit;
     }
     const uint32_t batch = batch_roots ? batch_roots : std::max<uint32_t>(1, (g->nl + 63) / 64);
     uint32_t batches = 0;

@@ -34,7 +34,8 @@ enum {
     GMK_E_OUTBUF = -9,   /* record buffer too small for emit mode; raise out_words */
     GMK_E_SINK = -10,    /* the sink asked to stop (not an error for the caller's data) */
     GMK_E_NODEV = -11,   /* no CUDA device / extension not usable */
-    GMK_E_CHECKPOINT = -12, /* checkpoint file unreadable, or written for another graph / k */
+    GMK_E_CHECKPOINT = -12, /* checkpoint file unreadable, or written for another run
+                               (graph, k, schedule, order, shard or result limit) */
     GMK_E_SCRATCH = -13, /* gmk_enumerate_noalloc: the request does not fit the static scratch */
     GMK_PAUSED = 1       /* not an error: max_batches reached, the checkpoint holds the rest */
 };
@@ -113,8 +114,13 @@ typedef struct {
 
 typedef struct {
     uint64_t count;           /* results (clamped to result_limit) */
-    uint64_t hash_sum;        /* wrapping sum of per-result h1 (exact only when not truncated) */
-    uint64_t hash_xor;        /* xor of per-result h2 (exact only when not truncated) */
+    uint64_t hash_sum;        /* wrapping sum of per-result h1 */
+    uint64_t hash_xor;        /* xor of per-result h2.  Both hashes describe the result set
+                                 only when truncated == 0.  A count-only run (emit = 0) that a
+                                 result_limit stopped counts results in batches per worker, so
+                                 its hashes may include results past the limit and are not a
+                                 summary of any particular `count` results; emit = 1 runs hash
+                                 exactly the delivered results. */
     uint64_t nodes;           /* search-tree nodes */
     uint64_t algo_bytes;      /* adjacency/counter bytes the search read (4 per word) */
     uint64_t tasks;           /* search tasks in the queue */
@@ -162,7 +168,8 @@ int gmk_enumerate_batch(gmk_graph* const* graphs, uint32_t n_graphs, const uint3
  * batch, atomically rewrites `checkpoint_path` with the next root position
  * and the running count and set hash.  If the file exists when the call
  * starts, the run resumes from it (it must have been written for the same
- * graph, k and schedule; else GMK_E_CHECKPOINT).  Results of finished batches
+ * graph, k, schedule, root order, shard and result limit; else
+ * GMK_E_CHECKPOINT).  Results of finished batches
  * are not delivered again.  With max_batches > 0 the call returns GMK_PAUSED
  * after that many batches if work remains.  *out holds the totals of the
  * whole run, resumed part included; a finished run leaves the file marked
@@ -178,24 +185,32 @@ int gmk_enumerate_resumable(gmk_graph* g, const gmk_opts* opts, const char* chec
  * footprint before the search starts).  The caller passes the graph as device
  * CSR arrays it owns (d_offsets: n+1 words, d_adj: d_offsets[n] words, rows
  * sorted, U rows hold V ids and vice versa) and receives the counts and set
- * hash in *out.  The search runs the one-task-per-thread engine with the batched
- * schedule; its arenas, member buffers and counters live in one static device
- * array of GMK_STATIC_SCRATCH_BYTES that every GPU loading libgmk.so holds until
- * the process exits.  Nothing is allocated: no cudaMalloc, no cudaFree, no events.
+ * hash in *out.  The CSR is checked on the device first (offsets from 0,
+ * non-decreasing and within d_offsets[n]; rows ascending; ids on the other
+ * side): a malformed one returns GMK_E_FORMAT before the search reads it.
+ * d_adj must really hold d_offsets[n] words; that cannot be checked.
+ * The search runs the one-task-per-thread engine with the batched schedule
+ * (no tree splitting); its arenas, member buffers and counters live in one
+ * static device array of GMK_STATIC_SCRATCH_BYTES that every GPU loading
+ * libgmk.so holds until the process exits.  The call itself allocates
+ * nothing: no cudaMalloc, no cudaFree, no events.
  *   threads:     search threads (0 = 2048), a multiple of 128 is used;
  *   arena_words: per-thread search arena in u32 words (0 = 4096);
  *   max_members: largest |X|+|Y| (0 = 512).
  * threads x (4 arena_words + 8 max_members) bytes plus 256 for the counters must
  * fit GMK_STATIC_SCRATCH_BYTES, else GMK_E_SCRATCH.  A search that outgrows its
- * arena returns GMK_E_ARENA as gmk_enumerate does.
- * The first call on a device looks up the array's device address (once per
- * device, with that device made current); make that first call before any
- * stream capture begins.  The call runs on `stream` (a cudaStream_t, NULL = the
- * legacy default stream) and returns after the search finished.  All calls on a
- * device share the one array, which keeps the last call's contents; each call
- * clears the counters it needs.  Calls that overlap on the GPU (from several
- * host threads or streams) race on the array and must be serialised by the
- * caller.  out->kernel_ms is host wall time of the launch and wait. */
+ * arena returns GMK_E_ARENA (gmk_enumerate would split the task instead).
+ * Set-up: the first call on a device looks up the array's device address
+ * (once per device, with that device made current).  Under CUDA's lazy module
+ * loading that first call may also be what loads libgmk's device code and so
+ * creates the array: make one call at initialisation (a warm-up on a tiny
+ * graph), before entering the code that must not allocate, and before any
+ * stream capture begins.  The call runs on `stream` (a cudaStream_t, NULL =
+ * the legacy default stream) and returns after the search finished.  All calls
+ * on a device share the one array, which keeps the last call's contents; each
+ * call clears the counters it needs.  Calls that overlap on the GPU (from
+ * several host threads or streams) race on the array and must be serialised by
+ * the caller.  out->kernel_ms is host wall time of the check, launch and wait. */
 #define GMK_STATIC_SCRATCH_BYTES (64u << 20)
 int gmk_enumerate_noalloc(const uint32_t* d_offsets, const uint32_t* d_adj, uint32_t n,
                           uint32_t n_left, uint32_t k, uint64_t result_limit, uint32_t threads,

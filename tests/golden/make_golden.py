@@ -1,6 +1,6 @@
 """Regenerate the golden fixtures under tests/golden/.
 
-Run in a checkout that has the reference tree at REF (default /root/reference)
+Run in a checkout that has the reference tree at $GMK_REFERENCE (oracle/refpath.py)
 and the BPPivot binary built by `make -C oracle ref`:
 
     python tests/golden/make_golden.py
@@ -32,7 +32,7 @@ import numpy as np  # noqa: E402
 import oracle as O  # noqa: E402
 from gmkbe_b200 import graphgen as gg  # noqa: E402
 
-REF = os.environ.get("GMK_REFERENCE", "/root/reference")
+from oracle.refpath import REFERENCE as REF  # noqa: E402
 FIXTURES = {
     "southernwomen": "baselines/MaximalBiPlex/datas/opsahl_southernwomen.txt",
     "crime": "baselines/MaximalBiPlex/datas/moreno_crime.txt",

@@ -12,6 +12,7 @@ import pytest
 from gmkbe_b200 import convert as C
 from gmkbe_b200 import graphgen as gg
 from conftest import ROOT, golden_graph_path
+from oracle.refpath import ref_path
 
 REF_CONVERT = os.path.join(ROOT, "oracle", "_ref", "graph_convert")
 needs_ref = pytest.mark.skipif(not os.path.exists(REF_CONVERT),
@@ -45,7 +46,7 @@ def test_golden_graphs_are_converter_ordered():
 @needs_ref
 @pytest.mark.parametrize("fixture", ["opsahl_southernwomen", "moreno_crime", "opsahl_ucforum"])
 def test_konect_fixtures_byte_identical(tmp_path, fixture):
-    src = os.path.join("/root/reference/baselines/MaximalBiPlex/datas", fixture + ".txt")
+    src = ref_path("baselines", "MaximalBiPlex", "datas", fixture + ".txt")
     if not os.path.exists(src):
         pytest.skip("reference fixtures absent")
     lines = open(src).read().splitlines()[1:]             # size header removed

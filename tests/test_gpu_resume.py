@@ -75,3 +75,21 @@ def test_result_limit_across_resume(tmp_path):
                                                result_limit=50_000)
         assert st.count == 50_000 and st.truncated
     assert os.path.exists(ck)
+
+
+def test_checkpoint_for_other_shard_or_limit_is_refused(tmp_path):
+    # a checkpoint records the task set it covers: shard, shard count and
+    # result limit must match, or counts from two task sets would mix
+    ck = str(tmp_path / "sh.ckpt")
+    with G.Graph.load(golden_graph_path("er60")) as g:
+        g.enumerate_resumable(ck, batch_roots=4, max_batches=1, k=1, shard=0, nshards=2)
+        text = open(ck).read()
+        assert "shard 0\nnshards 2\nresult_limit 0\n" in text
+        for kw in (dict(shard=1, nshards=2), dict(shard=0, nshards=3), dict(shard=0, nshards=1),
+                   dict(shard=0, nshards=2, result_limit=10)):
+            with pytest.raises(G.GmkError) as e:
+                g.enumerate_resumable(ck, batch_roots=4, k=1, **kw)
+            assert e.value.code == -12, kw
+        # the matching run resumes
+        st, paused = g.enumerate_resumable(ck, batch_roots=4, k=1, shard=0, nshards=2)
+        assert not paused and st.count > 0

@@ -6,7 +6,8 @@ and a C ABI (include/gmk.h, libgmk.so) for embedding.  The search runs only
 on the GPU; without the built library every entry point raises.
 """
 from .api import (EXPORTS, LIB_PATH, Graph, GmkError, Stats, enumerate_batch,  # noqa: F401
-                  load_library, result_hash)
+                  load_library, plan_tasks, result_hash)
 
-__all__ = ["Graph", "GmkError", "Stats", "enumerate_batch", "load_library", "result_hash",
+__all__ = ["Graph", "GmkError", "Stats", "enumerate_batch", "load_library", "plan_tasks",
+           "result_hash",
            "EXPORTS", "LIB_PATH"]

@@ -27,7 +27,8 @@ EXPORTS = ("gmk_graph_load", "gmk_graph_from_csr", "gmk_graph_info", "gmk_graph_
            "gmk_opts_default", "gmk_enumerate", "gmk_enumerate_batch", "gmk_enumerate_resumable",
            "gmk_enumerate_noalloc", "gmk_result_hash", "gmk_strerror", "gmk_last_cuda_error",
            "gmk_abi_version", "gmk_root_features", "gmk_mlp_create", "gmk_mlp_free",
-           "gmk_mlp_params", "gmk_mlp_gradient", "gmk_mlp_train", "gmk_mlp_predict")
+           "gmk_mlp_params", "gmk_mlp_gradient", "gmk_mlp_train", "gmk_mlp_predict",
+           "gmk_root_costs", "gmk_plan_tasks")
 
 SCHEDULES = {"plain": 0, "batched": 1, "ordered": 2}
 ENGINES = {"warp": 0, "thread": 1}
@@ -54,7 +55,9 @@ class _Opts(ctypes.Structure):
                 ("shard", ctypes.c_uint32), ("nshards", ctypes.c_uint32),
                 ("engine", ctypes.c_int32), ("split_min_nodes", ctypes.c_uint32),
                 ("root_begin", ctypes.c_uint32), ("root_end", ctypes.c_uint32),
-                ("root_nodes", ctypes.POINTER(ctypes.c_uint64))]
+                ("root_nodes", ctypes.POINTER(ctypes.c_uint64)),
+                ("donate_min_nodes", ctypes.c_uint32), ("no_sharing", ctypes.c_int32),
+                ("tasks", ctypes.c_void_p), ("n_tasks", ctypes.c_uint64)]
 
 
 class _Stats(ctypes.Structure):
@@ -63,7 +66,12 @@ class _Stats(ctypes.Structure):
                 ("algo_bytes", ctypes.c_uint64), ("tasks", ctypes.c_uint64),
                 ("tasks_done", ctypes.c_uint64), ("kernel_ms", ctypes.c_double),
                 ("truncated", ctypes.c_int32), ("threads", ctypes.c_uint32),
-                ("rounds", ctypes.c_uint32)]
+                ("rounds", ctypes.c_uint32), ("donations", ctypes.c_uint64)]
+
+
+class _Task(ctypes.Structure):
+    _fields_ = [("root", ctypes.c_uint32), ("first", ctypes.c_uint32), ("last", ctypes.c_uint32),
+                ("graph", ctypes.c_uint32), ("cost", ctypes.c_float)]
 
 
 SINK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32),
@@ -115,6 +123,11 @@ def load_library(path: str = LIB_PATH):
     lib.gmk_result_hash.argtypes = [P32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                                     ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
     lib.gmk_result_hash.restype = None
+    lib.gmk_root_costs.argtypes = [ctypes.c_void_p, PF]
+    lib.gmk_plan_tasks.argtypes = [ctypes.c_uint32, ctypes.c_uint32, PF, ctypes.c_uint32,
+                                   ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint32,
+                                   ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(_Task),
+                                   ctypes.POINTER(ctypes.c_uint64)]
     lib.gmk_strerror.restype = ctypes.c_char_p
     lib.gmk_last_cuda_error.restype = ctypes.c_char_p
     _lib = lib
@@ -141,6 +154,7 @@ class Stats:
     threads: int
     rounds: int = 1
     results: list | None = None
+    donations: int = 0
 
     def summary(self) -> tuple[int, int, int]:
         return self.count, self.hash_sum, self.hash_xor
@@ -173,6 +187,29 @@ def enumerate_batch(graphs, ks, schedule: str = "batched", task_costs=None, **tu
     return [Graph._stats(outs[i], None) for i in range(n)]
 
 
+def plan_tasks(n: int, n_left: int, root_cost, root_begin: int = 0, root_end: int | None = None,
+               target_tasks: int = 1, max_chunks: int = 0, nshards: int = 1,
+               shard: int = 0) -> np.ndarray:
+    """gmk_plan_tasks (host only, no GPU needed): this shard's planned tasks as
+    a structured array with fields root, first, last, graph, cost, largest
+    cost first."""
+    lib = load_library()
+    cost = np.ascontiguousarray(root_cost, dtype=np.float32)
+    if cost.size != n_left:
+        raise ValueError("root_cost needs one value per U vertex")
+    re_ = n_left if root_end is None else root_end
+    PF = ctypes.POINTER(ctypes.c_float)
+    cnt = ctypes.c_uint64()
+    args = (n, n_left, cost.ctypes.data_as(PF), root_begin, re_, target_tasks, max_chunks,
+            nshards, shard)
+    _check(lib.gmk_plan_tasks(*args, None, ctypes.byref(cnt)))
+    buf = (_Task * max(1, cnt.value))()
+    _check(lib.gmk_plan_tasks(*args, buf, ctypes.byref(cnt)))
+    dt = np.dtype([("root", np.uint32), ("first", np.uint32), ("last", np.uint32),
+                   ("graph", np.uint32), ("cost", np.float32)])
+    return np.frombuffer(bytes(buf), dtype=dt, count=cnt.value).copy()
+
+
 def result_hash(x, y) -> tuple[int, int]:
     """The library's per-result hash pair (gmk_result_hash)."""
     lib = load_library()
@@ -193,6 +230,12 @@ class Graph:
         n, nl, m = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint64()
         _check(lib.gmk_graph_info(self._h, ctypes.byref(n), ctypes.byref(nl), ctypes.byref(m)))
         self.n, self.n_left, self.adj_len = n.value, nl.value, m.value
+
+    def root_costs(self) -> np.ndarray:
+        """gmk_root_costs: the 2-hop cost proxy of every root (float32, n_left)."""
+        out = np.zeros(self.n_left, np.float32)
+        _check(load_library().gmk_root_costs(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return out
 
     def fingerprint(self) -> int:
         """64-bit hash of the CSR (the identity checkpoints and tuning caches record)."""
@@ -280,14 +323,15 @@ class Graph:
     def _stats(st, results):
         return Stats(st.count, st.hash_sum, st.hash_xor, st.nodes, st.algo_bytes, st.tasks,
                      st.tasks_done, st.kernel_ms, bool(st.truncated), st.threads, st.rounds,
-                     results)
+                     results, st.donations)
 
     def enumerate(self, k: int = 1, result_limit: int = 0, schedule: str = "batched",
                   collect: bool = False, chunk: int = 0, threads: int = 0, arena_words: int = 0,
                   max_members: int = 0, watchdog_ms: int = 0, pair_limit: int = 0,
                   task_cost=None, sink=None, shard: int = 0, nshards: int = 1,
                   engine: str = "warp", split_min_nodes: int = 0, root_begin: int = 0,
-                  root_end: int = 0, root_nodes=None, out_words: int = 0) -> Stats:
+                  root_end: int = 0, root_nodes=None, out_words: int = 0,
+                  donate_min_nodes: int = 0, sharing: bool = True, tasks=None) -> Stats:
         """Enumerate maximal k-biplexes.  collect=True returns the result list
         (sorted X, Y tuples) in Stats.results; `sink(x, y)` is called per
         result otherwise (return True to stop).  root_nodes: a uint64 numpy
@@ -301,6 +345,18 @@ class Graph:
                     not root_nodes.flags.c_contiguous:
                 raise ValueError("root_nodes must be a contiguous uint64 array of n_left entries")
             o.root_nodes = root_nodes.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+        o.donate_min_nodes = donate_min_nodes
+        o.no_sharing = 0 if sharing else 1
+        task_buf = None
+        if tasks is not None:
+            # an explicit task list (structured array from plan_tasks, or rows of
+            # (root, first, last)): run exactly these tasks
+            rows = [(int(t[0]), int(t[1]), int(t[2])) for t in tasks]
+            task_buf = (_Task * max(1, len(rows)))()
+            for i, (r, f, l) in enumerate(rows):
+                task_buf[i] = _Task(r, f, l, 0, 0.0)
+            o.tasks = ctypes.cast(task_buf, ctypes.c_void_p)
+            o.n_tasks = len(rows)
         out: list = []
         cb = self._sink(collect, sink, out)
         o.emit = 1 if (collect or sink is not None) else 0

@@ -1388,6 +1388,126 @@ __device__ bool split_path(Ctx& t, const SplitBuf& sb, uint32_t cur) {
     return true;
 }
 
+// ----------------------------------------------------------------- work sharing
+
+// In-launch work sharing.  A warp that runs out of tasks registers as idle;
+// a busy warp that sees idle warps (at its poll points) donates the shallowest
+// frame of its path that still has unexplored children -- the largest piece of
+// its remaining tree -- as a record in the same format as split_path's, and
+// marks that frame finished in its own stack.  Idle warps take records in
+// order.  `outstanding` counts the launch's unfinished tasks (the queue's
+// entries plus the donations, minus the finished), kept offset by the queue
+// length: the launch's work is done when it returns to -queue_len.  Records
+// live in a bump-allocated buffer for the launch; once it is full, donation
+// stops and the busy warps split into the next round as before.
+struct Donation {
+    uint32_t* words;
+    unsigned long long word_cap;
+    unsigned long long* idx;          // slot -> record offset + 1 (0: not yet written)
+    unsigned long long idx_cap;
+    unsigned long long* used;         // words reserved
+    unsigned long long* tail;         // slots reserved
+    unsigned long long* head;         // slots taken
+    unsigned long long* outstanding;  // unfinished tasks - queue_len (mod 2^64)
+    unsigned long long* beat;         // busy warps' heartbeat while others wait
+    unsigned long long* donated;      // records published (statistics)
+    unsigned int* idle;               // warps waiting for a record
+    int* full;                        // a reservation failed: no more donations
+    uint32_t min_nodes;               // a task donates only after this many nodes
+};
+
+// Is there anything left to iterate in entered frame f (phase < 2)?  Exact
+// for the sides' positions; the "U child needs a V member" rule of phase 1 is
+// left to the taker (it then finds nothing).
+__device__ __forceinline__ bool frame_has_more(const GraphView& g, const uint32_t* f) {
+    const uint32_t phase = f[F_PHASE];
+    if (phase >= 2) return false;
+    const uint32_t order = f[F_ORDER];
+    const int s = phase == 0 ? (int)order : 1 - (int)order;
+    const bool gl = f[F_FLAGS] & (s ? FL_G1 : FL_G0);
+    const uint32_t limit = gl ? (phase == 0 && f[F_END] < side_end(g, s) ? f[F_END] : side_end(g, s))
+                              : f[F_CNT0 + s];
+    if (f[F_POS] < limit) return true;
+    if (phase == 1) return false;
+    const int s2 = 1 - s;
+    if (f[F_FLAGS] & (s2 ? FL_G1 : FL_G0)) return f[F_LO0 + s2] + 1 < side_end(g, s2);
+    return f[F_CNT0 + s2] > 0;
+}
+
+// Donates the shallowest pending frame above or at `cur` (entered frames
+// only).  Returns true when a record was published.  Inlined: an out-of-line
+// call makes the search loop save its live registers around the call site
+// (ptxas: 48 -> 270 bytes of stack and 5x the spill loads).
+__device__ __forceinline__ bool donate_top(Ctx& t, const Donation& db, uint32_t cur) {
+    uint32_t best = kNoPos;
+    #pragma unroll 1
+    for (uint32_t x = cur; x != kNoPos; x = t.arena[x + F_PARENT_SLOT]) {
+        const uint32_t* f = t.arena + x;
+        if ((f[F_FLAGS] & FL_ENTERED) && frame_has_more(t.g, f)) best = x;
+    }
+    if (best == kNoPos) return false;
+    const uint32_t* f = t.arena + best;
+    const uint32_t ns = f[F_NS];
+    const uint32_t c0 = (f[F_FLAGS] & FL_G0) ? 0u : f[F_CNT0];
+    const uint32_t c1 = (f[F_FLAGS] & FL_G1) ? 0u : f[F_CNT1];
+    const unsigned long long words = kRecHeader + 2ull * ns + F_WORDS + 2ull * (c0 + c1);
+    unsigned long long w0 = 0, slot = 0;
+    int ok = 0;
+    if (t.lane == 0) {
+        w0 = atomicAdd(db.used, words);
+        if (w0 + words <= db.word_cap) {
+            slot = atomicAdd(db.tail, 1ull);
+            ok = slot < db.idx_cap;
+        }
+        if (!ok) atomicExch(db.full, 1);
+    }
+    if (!bcast(ok)) return false;
+    w0 = bcast(w0);
+    slot = bcast(slot);
+    uint32_t* r = db.words + w0;
+    if (t.lane == 0) { r[0] = ns; r[1] = c0; r[2] = c1; r[3] = t.gid; }
+    uint32_t* rs = r + kRecHeader;
+    // members as of the frame, with their misses at that depth: the deeper
+    // members' misses are taken off (recorded masks where they exist, else
+    // adjacency tests), so the warp's own S stays as it is
+    #pragma unroll 1
+    for (uint32_t i = t.lane; i < ns; i += 32) {
+        const uint32_t m = t.sid[i];
+        const int sm = side_of(t.g, m);
+        uint32_t miss = t.smc[i];
+        #pragma unroll 1
+        for (uint32_t j = ns; j < t.ns; ++j) {
+            if (j <= 32 && j >= t.mask_base) {
+                miss -= (i < 32 && ((t.smask[j] >> i) & 1u)) ? 1u : 0u;
+            } else {
+                const uint32_t c = t.sid[j];
+                if (side_of(t.g, c) != sm && !adj_test(t, c, m)) --miss;
+            }
+        }
+        rs[i] = m;
+        rs[ns + i] = miss;
+    }
+    uint32_t* fr = rs + 2 * ns;
+    if (t.lane < F_WORDS) fr[t.lane] = f[t.lane];
+    uint32_t* lr = fr + F_WORDS;
+    const uint32_t* a0 = t.arena + f[F_OFF0];
+    const uint32_t* a1 = t.arena + f[F_OFF1];
+    #pragma unroll 1
+    for (uint32_t i = t.lane; i < 2 * c0; i += 32) lr[i] = a0[i];
+    #pragma unroll 1
+    for (uint32_t i = t.lane; i < 2 * c1; i += 32) lr[2 * c0 + i] = a1[i];
+    __syncwarp();
+    if (t.lane == 0) {
+        atomicAdd(db.outstanding, 1ull);   // before the record can be taken and finished
+        atomicAdd(db.donated, 1ull);
+        __threadfence();
+        atomicExch(db.idx + slot, w0 + 1);
+        t.arena[best + F_PHASE] = 2;       // the rest of this frame is the record's now
+    }
+    __syncwarp();
+    return true;
+}
+
 // ----------------------------------------------------------------- tasks
 
 struct RunLimits {
@@ -1409,7 +1529,8 @@ __device__ __forceinline__ bool draining(const RunLimits& lim) {
 // entered.
 template <bool kRec, bool kBits>
 __device__ __forceinline__ unsigned long long run_dfs(Ctx& t, const Outputs& o, uint32_t first,
-                                                     const SplitBuf* sb, const RunLimits& lim) {
+                                                     const SplitBuf* sb, const RunLimits& lim,
+                                                     const Donation* db) {
     uint32_t cur = 0;
     uint32_t polls = 0;
     unsigned long long task_nodes = 0;
@@ -1420,18 +1541,31 @@ __device__ __forceinline__ unsigned long long run_dfs(Ctx& t, const Outputs& o, 
 #define GMK_POLL_MASK 15u    // stop / watchdog / split checks every 16 loop steps
 #endif
         if ((++polls & GMK_POLL_MASK) == 0) {
-            int stop = 0, late = 0, hungry = 0;
+            int stop = 0, late = 0, hungry = 0, give = 0;
             if (t.lane == 0) {
                 stop = load_flag(o.stop);
                 late = o.deadline_ns && now_ns() > o.deadline_ns;
+                // in-launch sharing while its buffer has room; splitting into
+                // the next round otherwise
+                const bool share = !kRec && db && !load_flag(db->full);
+                if (share) {
+                    const unsigned idle = *(volatile const unsigned*)db->idle;
+                    if (idle) {
+                        atomicAdd(db->beat, 1ull);
+                        const unsigned long long avail = *(volatile const unsigned long long*)db->tail -
+                                                         *(volatile const unsigned long long*)db->head;
+                        give = task_nodes >= db->min_nodes && avail < idle;
+                    }
+                }
                 hungry = may_split && task_nodes >= 1 &&
-                         ((lim.split_min_nodes && task_nodes >= lim.split_min_nodes &&
+                         ((!share && lim.split_min_nodes && task_nodes >= lim.split_min_nodes &&
                            *(volatile const unsigned long long*)lim.queue >= lim.queue_len) ||
                           (kRec && draining(lim)));
             }
-            stop = bcast(stop); late = bcast(late); hungry = bcast(hungry);
+            stop = bcast(stop); late = bcast(late); hungry = bcast(hungry); give = bcast(give);
             if (stop) break;
             if (late) { fail(t, o, TASK_E_TIMEOUT); break; }
+            if (!kRec && give) donate_top(t, *db, cur);
             if (hungry) {
                 if (split_path(t, *sb, cur)) break;
                 may_split = false;   // buffer full: finish this task here
@@ -1477,7 +1611,8 @@ __device__ __forceinline__ unsigned long long run_dfs(Ctx& t, const Outputs& o, 
 // Root task: x in U with its first-level children y in [first, last).
 template <bool kRec, bool kBits>
 __device__ unsigned long long run_root(Ctx& t, const Outputs& o, uint32_t root, uint32_t first,
-                                       uint32_t last, const SplitBuf* sb, const RunLimits& lim) {
+                                       uint32_t last, const SplitBuf* sb, const RunLimits& lim,
+                                       const Donation* db) {
     t.ns = 0; t.nss.a = t.nss.b = 0;
     t.mask_base = 0;
     push_member(t, root, nullptr);
@@ -1496,14 +1631,17 @@ __device__ unsigned long long run_root(Ctx& t, const Outputs& o, uint32_t root, 
         }
     if (t.lane == 0) write_hdr(t.arena, h);
     __syncwarp();
-    return run_dfs<kRec, kBits>(t, o, first, sb, lim);
+    return run_dfs<kRec, kBits>(t, o, first, sb, lim, db);
 }
 
-// Resumed task: a frame written by split_path (its S starts with the root).
+// Resumed task: a frame written by split_path or donate_top (its S starts
+// with the root).  Records are read with L2-coherent loads (__ldcg): a
+// donated one was written moments ago by a warp on another SM.
 template <bool kRec, bool kBits>
 __device__ unsigned long long run_record(Ctx& t, const Outputs& o, const uint32_t* r,
-                                         const SplitBuf* sb, const RunLimits& lim) {
-    const uint32_t ns = r[0], c0 = r[1], c1 = r[2];
+                                         const SplitBuf* sb, const RunLimits& lim,
+                                         const Donation* db) {
+    const uint32_t ns = __ldcg(r), c0 = __ldcg(r + 1), c1 = __ldcg(r + 2);
     if (ns > t.smax) { fail(t, o, TASK_E_SMAX); return 0; }
     if (F_WORDS + 2ull * (c0 + c1) > t.cap) { fail(t, o, TASK_E_ARENA); return 0; }
     uint32_t nv = 0;
@@ -1513,9 +1651,9 @@ __device__ unsigned long long run_record(Ctx& t, const Outputs& o, const uint32_
         const uint32_t i = base + t.lane;
         bool isv = false;
         if (i < ns) {
-            const uint32_t v = rs[i];
+            const uint32_t v = __ldcg(rs + i);
             t.sid[i] = v;
-            t.smc[i] = rs[ns + i];
+            t.smc[i] = __ldcg(rs + ns + i);
             isv = side_of(t.g, v) != 0;
         }
         nv += __popc(__ballot_sync(kFull, isv));
@@ -1523,7 +1661,12 @@ __device__ unsigned long long run_record(Ctx& t, const Outputs& o, const uint32_
     t.ns = ns; t.nss.b = nv; t.nss.a = ns - nv;
     t.mask_base = ns;
     const uint32_t* fr = rs + 2 * ns;
-    Hdr h = read_hdr(fr);
+    Hdr h;
+    h.ns = __ldcg(fr + F_NS); h.flags = __ldcg(fr + F_FLAGS);
+    h.lo.a = __ldcg(fr + F_LO0); h.lo.b = __ldcg(fr + F_LO1);
+    h.order = __ldcg(fr + F_ORDER); h.phase = __ldcg(fr + F_PHASE); h.pos = __ldcg(fr + F_POS);
+    h.end = __ldcg(fr + F_END);
+    h.cnt.a = c0; h.cnt.b = c1;
     h.flags &= ~(FL_BITS0 | FL_BITS1);   // bitmaps are not part of a record
     h.off.a = F_WORDS;
     h.off.b = F_WORDS + 2 * c0;
@@ -1531,10 +1674,10 @@ __device__ unsigned long long run_record(Ctx& t, const Outputs& o, const uint32_
     h.parent = kNoPos;
     const uint32_t* lr = fr + F_WORDS;
     #pragma unroll 1
-    for (uint32_t i = t.lane; i < 2 * (c0 + c1); i += 32) t.arena[F_WORDS + i] = lr[i];
+    for (uint32_t i = t.lane; i < 2 * (c0 + c1); i += 32) t.arena[F_WORDS + i] = __ldcg(lr + i);
     if (t.lane == 0) write_hdr(t.arena, h);
     __syncwarp();
-    return run_dfs<kRec, kBits>(t, o, 0, sb, lim);
+    return run_dfs<kRec, kBits>(t, o, 0, sb, lim, db);
 }
 
 }  // namespace warp

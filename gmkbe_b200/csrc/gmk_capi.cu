@@ -57,6 +57,10 @@ struct RoundCounters {
     unsigned long long next_fail;   // lowest split-record index that found no room (~0: none)
     int split_refused;              // first reason a split was refused (0 = none)
     int pad;
+    // in-launch work sharing (gmk::warp::Donation)
+    unsigned long long dq_used, dq_tail, dq_head, outstanding, beat, donated;
+    unsigned int idle;
+    int dq_full;
 };
 
 constexpr int kBlock = 128;
@@ -68,13 +72,18 @@ constexpr uint32_t kDefaultSmax = 2048;
 #endif
 constexpr uint32_t kDefaultPairLimit = GMK_PAIR_LIMIT;
 
+// A planned search task (gmk_plan_tasks): root x and the first-level V
+// children [first, last) of its search.
+struct TaskEntry {
+    uint32_t root, first, last, pad;
+};
+
 __global__ void __launch_bounds__(kBlock)
 enumerate_kernel(gmk::GraphView g, uint32_t k, Counters* ctr, uint32_t* arenas,
                  uint32_t arena_words, uint32_t* sbuf, uint32_t smax, uint32_t pair_limit,
                  unsigned long long n_tasks, uint32_t chunk, uint32_t chunks_per_root,
-                 const uint32_t* root_order, uint32_t root_base, unsigned long long limit,
-                 uint32_t* out_buf, unsigned long long out_cap, unsigned long long watchdog_ns,
-                 uint32_t shard, uint32_t nshards) {
+                 const TaskEntry* tasks, uint32_t root_base, unsigned long long limit,
+                 uint32_t* out_buf, unsigned long long out_cap, unsigned long long watchdog_ns) {
     const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     gmk::Outputs o;
     o.count = &ctr->count; o.hash_sum = &ctr->hash_sum; o.hash_xor = &ctr->hash_xor;
@@ -90,16 +99,20 @@ enumerate_kernel(gmk::GraphView g, uint32_t k, Counters* ctr, uint32_t* arenas,
     t.scan_limit = pair_limit; t.err = 0;
     t.cnt = t.hsum = t.hxor = t.nodes = t.work = 0;
     while (!gmk::load_flag(o.stop)) {
-        const unsigned long long j = atomicAdd(&ctr->next_task, 1ull);
-        const unsigned long long id = j * nshards + shard;
+        const unsigned long long id = atomicAdd(&ctr->next_task, 1ull);
         if (id >= n_tasks) break;
         atomicAdd(&ctr->tasks_done, 1ull);
-        const uint32_t r = root_base + (uint32_t)(id / chunks_per_root);
-        const uint32_t c = (uint32_t)(id % chunks_per_root);
-        const uint32_t root = root_order ? root_order[r] : r;
-        const uint32_t first = g.nl + c * chunk;
-        const uint64_t end = (uint64_t)first + chunk;
-        const uint32_t last = end < g.n ? (uint32_t)end : g.n;
+        uint32_t root, first, last;
+        if (tasks) {
+            const TaskEntry e = tasks[id];
+            root = e.root; first = e.first; last = e.last;
+        } else {
+            root = root_base + (uint32_t)(id / chunks_per_root);
+            const uint32_t c = (uint32_t)(id % chunks_per_root);
+            first = g.nl + c * chunk;
+            const uint64_t end = (uint64_t)first + chunk;
+            last = end < g.n ? (uint32_t)end : g.n;
+        }
         gmk::run_task(t, o, root, first, last);
         gmk::flush(t, o);
         if (t.err) break;
@@ -129,6 +142,12 @@ constexpr int kWarpsPerBlock = kWBlock / 32;
 // faster than 25.
 constexpr int kBatchMinBlocks = 20;
 constexpr uint32_t kDefaultWarpArena = 1u << 18;
+// In-launch sharing: a task donates only after this many nodes of its own
+// (gmk_opts.donate_min_nodes 0).
+#ifndef GMK_DONATE_MIN
+#define GMK_DONATE_MIN 16
+#endif
+constexpr uint32_t kDefaultDonateMin = GMK_DONATE_MIN;
 
 // One graph of a launch.  A launch enumerates one graph (gmk_enumerate) or a
 // batch of graphs (gmk_enumerate_batch); each has its own k, chunking, root
@@ -139,7 +158,6 @@ struct GraphTask {
     gmk::warp::EdgeHash eh;
     uint32_t k;
     uint32_t chunk, n_roots, root_base;
-    const uint32_t* root_order;
     Counters* ctr;                     // counts, hashes, nodes, work of this graph
     unsigned long long* root_nodes;    // optional per-root node log
     unsigned long long task_begin;
@@ -170,8 +188,17 @@ struct WarpArgs {
     uint32_t* out_buf;
     unsigned long long out_cap;
     unsigned long long watchdog_ns;
-    uint32_t shard, nshards;
+    const TaskEntry* tasks;            // planned root tasks (pad = graph), or null: each
+                                       // graph's roots chunk-major (GraphTask)
+    gmk::warp::Donation share;         // in-launch work sharing (share.words null: off)
 };
+
+// An idle warp gives up when no busy warp has shown a sign of life (a
+// heartbeat at its poll points) for this long: a safety net that turns a
+// lost task into an error instead of a kernel that never ends.
+constexpr unsigned long long kIdleLimitNs = 10ull * 1000000000ull;
+// Longest wait for a reserved record to be published by its writer.
+constexpr unsigned long long kPublishLimitNs = 1000000000ull;
 
 // Points the warp's context and counters at graph gid of the launch.  A
 // one-graph launch reads its graph from the kernel parameters, so the values
@@ -193,7 +220,7 @@ __device__ __forceinline__ const GraphTask& use_graph(const WarpArgs& a, uint32_
 // count-only instantiation carries none of the record and drain code).
 template <bool kBatch, bool kRec, bool kBits>
 __global__ void __launch_bounds__(kWBlock, kBatch ? kBatchMinBlocks : GMK_WARP_MIN_BLOCKS)
-enumerate_warp_kernel(const WarpArgs a) {
+enumerate_warp_kernel(const __grid_constant__ WarpArgs a) {
     __shared__ uint32_t s_sat[kWarpsPerBlock][gmk::kSatCap];
     __shared__ uint32_t s_src[kWarpsPerBlock][gmk::warp::kSrcCap];
     using namespace gmk::warp;
@@ -233,6 +260,7 @@ enumerate_warp_kernel(const WarpArgs a) {
     lim.out_pos = &a.rc->out_pos;
     lim.drain_at = a.drain_at;
     const SplitBuf* sb = (a.split_min_nodes || a.drain_at) ? &a.next : nullptr;
+    const Donation* db = (!kRec && a.share.words) ? &a.share : nullptr;
     for (;;) {
         unsigned long long j = ~0ull;
         int stop = 0;
@@ -259,41 +287,119 @@ enumerate_warp_kernel(const WarpArgs a) {
         }
         stop = bcast(stop);
         j = bcast(j);
-        if (stop || j >= a.queue_len) break;
-        if (lane == 0) atomicAdd(&a.rc->tasks_done, 1ull);
-        if (j >= a.n_records) {
-            const unsigned long long id = (a.root_task_base + (j - a.n_records)) * a.nshards + a.shard;
-            // the graph whose task range holds id (the last with task_begin <= id)
-            uint32_t lo = 0;
-            if (kBatch) {
-                uint32_t hi = a.n_graphs;
-                while (hi - lo > 1) {
-                    const uint32_t mid = (lo + hi) >> 1;
-                    if (a.graphs[mid].task_begin <= id) lo = mid; else hi = mid;
+        if (stop) break;
+        if (j >= a.queue_len) {
+            // the queue is empty: wait for a donated record, or for the end
+            // of the launch's work (no task outstanding)
+            if (!db) break;
+            unsigned long long slot = ~0ull, w = 0;
+            int quit = 0;
+            if (lane == 0) {
+                atomicAdd(db->idle, 1u);
+                unsigned long long last_beat = *(volatile unsigned long long*)db->beat;
+                unsigned long long t_beat = gmk::now_ns();
+                unsigned sleep_ns = 32;
+                for (;;) {
+                    if (gmk::load_flag(o.stop)) { quit = 1; break; }
+                    const unsigned long long h = *(volatile unsigned long long*)db->head;
+                    const unsigned long long tl = *(volatile unsigned long long*)db->tail;
+                    if (h < (tl < db->idx_cap ? tl : db->idx_cap)) {
+                        if (atomicCAS(db->head, h, h + 1) == h) { slot = h; break; }
+                        continue;
+                    }
+                    if (*(volatile unsigned long long*)db->outstanding + a.queue_len == 0) {
+                        quit = 1;
+                        break;
+                    }
+                    const unsigned long long b = *(volatile unsigned long long*)db->beat;
+                    const unsigned long long now = gmk::now_ns();
+                    if (b != last_beat) {
+                        last_beat = b;
+                        t_beat = now;
+                    } else if (now - t_beat > kIdleLimitNs) {
+                        atomicCAS(o.error, 0, gmk::TASK_E_TIMEOUT);
+                        atomicExch(o.stop, 1);
+                        quit = 1;
+                        break;
+                    }
+                    __nanosleep(sleep_ns);
+                    sleep_ns = sleep_ns < 2048 ? sleep_ns * 2 : sleep_ns;
+                }
+                atomicSub(db->idle, 1u);
+                if (slot != ~0ull) {
+                    // the writer reserved the slot with its words: it publishes shortly
+                    const unsigned long long t0 = gmk::now_ns();
+                    for (;;) {
+                        w = *(volatile unsigned long long*)(db->idx + slot);
+                        if (w) break;
+                        if (gmk::now_ns() - t0 > kPublishLimitNs) {
+                            atomicCAS(o.error, 0, gmk::TASK_E_TIMEOUT);
+                            atomicExch(o.stop, 1);
+                            quit = 1;
+                            break;
+                        }
+                        __nanosleep(64);
+                    }
+                    __threadfence();
                 }
             }
-            const GraphTask& G = use_graph<kBatch>(a, lo, t, o);
-            // chunk-major: every root's first chunk of children, then every
-            // root's second, ... (the low-degree V children come first)
-            const unsigned long long local = id - G.task_begin;
-            const uint32_t r = G.root_base + (uint32_t)(local % G.n_roots);
-            const uint32_t c = (uint32_t)(local / G.n_roots);
-            const uint32_t root = G.root_order ? G.root_order[r] : r;
-            const uint32_t first = t.g.nl + c * G.chunk;
-            const unsigned long long end = (unsigned long long)first + G.chunk;
-            const uint32_t last = end < t.g.n ? (uint32_t)end : t.g.n;
-            const unsigned long long nodes = run_root<kRec, kBits>(t, o, root, first, last, sb, lim);
+            quit = bcast(quit);
+            if (quit) break;
+            w = bcast(w);
+            const uint32_t* rec = db->words + (w - 1);
+            const GraphTask& G = use_graph<kBatch>(a, kBatch ? __ldcg(rec + 3) : 0u, t, o);
+            const unsigned long long nodes = run_record<kRec, kBits>(t, o, rec, sb, lim, db);
+            if (G.root_nodes && lane == 0)
+                atomicAdd(G.root_nodes + __ldcg(rec + gmk::warp::kRecHeader), nodes);
+            if (lane == 0) atomicAdd(db->outstanding, ~0ull);   // this record is finished
+            flush(t, o);
+            if (t.err) break;
+            continue;
+        }
+        if (lane == 0) atomicAdd(&a.rc->tasks_done, 1ull);
+        if (j >= a.n_records) {
+            const unsigned long long id = a.root_task_base + (j - a.n_records);
+            uint32_t root, first, last, gi = 0;
+            TaskEntry e{0, 0, 0, 0};
+            if (a.tasks) {
+                // planned: per-root chunks in proportion to the predicted
+                // cost, largest first (plan_tasks)
+                e = a.tasks[id];
+                gi = e.pad;
+            } else if (kBatch) {
+                // the graph whose task range holds id (the last with task_begin <= id)
+                uint32_t hi = a.n_graphs;
+                while (hi - gi > 1) {
+                    const uint32_t mid = (gi + hi) >> 1;
+                    if (a.graphs[mid].task_begin <= id) gi = mid; else hi = mid;
+                }
+            }
+            const GraphTask& G = use_graph<kBatch>(a, gi, t, o);
+            if (a.tasks) {
+                root = e.root; first = e.first; last = e.last;
+            } else {
+                // chunk-major: every root's first chunk of children, then
+                // every root's second, ... (the low-degree V children first)
+                const unsigned long long local = id - G.task_begin;
+                root = G.root_base + (uint32_t)(local % G.n_roots);
+                const uint32_t c = (uint32_t)(local / G.n_roots);
+                first = t.g.nl + c * G.chunk;
+                const unsigned long long end = (unsigned long long)first + G.chunk;
+                last = end < t.g.n ? (uint32_t)end : t.g.n;
+            }
+            const unsigned long long nodes = run_root<kRec, kBits>(t, o, root, first, last, sb, lim, db);
             if (G.root_nodes && lane == 0) atomicAdd(G.root_nodes + root, nodes);
         } else {
             const uint32_t* rec = a.cur_words + a.cur_idx[j];
             const GraphTask& G = use_graph<kBatch>(a, kBatch ? rec[3] : 0u, t, o);
             // a round that winds down hands its queued records on unchanged
             if (!(kRec && sb && draining(lim) && forward_record(t, *sb, rec))) {
-                const unsigned long long nodes = run_record<kRec, kBits>(t, o, rec, sb, lim);
+                const unsigned long long nodes = run_record<kRec, kBits>(t, o, rec, sb, lim, db);
                 if (G.root_nodes && lane == 0)
                     atomicAdd(G.root_nodes + rec[gmk::warp::kRecHeader], nodes);
             }
         }
+        if (db && lane == 0) atomicAdd(db->outstanding, ~0ull);   // this task is finished
         flush(t, o);
         if (t.err) break;
     }
@@ -332,6 +438,22 @@ __global__ void csr_check_kernel(const uint32_t* off, const uint32_t* adj, uint3
     if ((threadIdx.x & 31u) == 0 && h) atomicAdd(fp, h);
 }
 
+// Cost proxy of every root task x (one warp per root): 1 + the sum over its
+// neighbours y of |N(y) above x| -- the U vertices that can join x through a
+// common neighbour, i.e. the 2-hop candidates of the task.  The schedule's
+// default when no learned cost is given.
+__global__ void root_cost_kernel(gmk::GraphView g, float* out) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t x = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (x >= g.nl) return;
+    const uint32_t d = gmk::degree(g, (uint32_t)x);
+    const uint32_t* row = g.adj + g.off[x];
+    unsigned long long above = 0, words = 0;
+    for (uint32_t i = lane; i < d; i += 32) above += gmk::count_above(g, row[i], (uint32_t)x, &words);
+    for (int o = 16; o; o >>= 1) above += __shfl_xor_sync(0xFFFFFFFFu, above, o);
+    if (lane == 0) out[x] = 1.f + (float)above;
+}
+
 bool read_file(const char* path, std::vector<uint32_t>& words) {
     FILE* fp = std::fopen(path, "rb");
     if (!fp) return false;
@@ -364,6 +486,10 @@ struct gmk_graph {
     size_t eh_bytes = 0;
     unsigned long long* d_root_nodes = nullptr;   // per-root node log (on demand)
     __half* d_feat = nullptr;                     // root features (on demand)
+    float* d_cost = nullptr;                      // root cost proxy (on demand)
+    std::vector<float> cost;                      // its host copy, computed once
+    TaskEntry* d_tasks = nullptr;                 // planned task table (grown on demand)
+    size_t tasks_bytes = 0;
     RoundCounters* d_rc = nullptr;
     cudaStream_t stream = nullptr;
     cudaStream_t copy_stream = nullptr;   // record delivery, overlapping the next round
@@ -390,6 +516,13 @@ struct Workspace {
     size_t split_words_bytes[2] = {0, 0};
     unsigned long long* d_split_idx[2] = {nullptr, nullptr};
     size_t split_idx_bytes[2] = {0, 0};
+    // in-launch work sharing: donated records and their slot index (slots the
+    // last launch may have written are cleared before the next one)
+    uint32_t* d_dq_words = nullptr;
+    size_t dq_words_bytes = 0;
+    unsigned long long* d_dq_idx = nullptr;
+    size_t dq_idx_bytes = 0;
+    unsigned long long dq_dirty = 0;
 };
 constexpr int kMaxDevices = 64;
 Workspace g_ws[kMaxDevices];
@@ -699,7 +832,8 @@ void gmk_graph_free(gmk_graph* g) {
     pool_free(d, g->d_ctr, sizeof(Counters));
     pool_free(d, g->d_rc, sizeof(RoundCounters));
     pool_free(d, g->d_eh, g->eh_bytes);
-    cudaFree(g->d_order); cudaFree(g->d_root_nodes); cudaFree(g->d_feat);
+    cudaFree(g->d_order); cudaFree(g->d_root_nodes); cudaFree(g->d_feat); cudaFree(g->d_cost);
+    cudaFree(g->d_tasks);
     pool_return(d, g->stream, g->ev0);
     pool_return(d, g->copy_stream, g->ev1);
     delete g;
@@ -715,6 +849,77 @@ void gmk_opts_default(gmk_opts* o) {
 }  // extern "C"
 
 namespace {
+
+// Root costs of the proxy (root_cost_kernel), computed once per graph.
+int proxy_costs(gmk_graph* g, const float** out) {
+    if (g->cost.size() != g->nl) {
+        if (!g->d_cost) CK(cudaMalloc(&g->d_cost, 4ull * std::max<uint32_t>(g->nl, 1)));
+        gmk::GraphView gv{g->d_off, g->d_adj, g->n, g->nl};
+        const uint64_t threads = (uint64_t)g->nl * 32;
+        root_cost_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, g->stream>>>(gv, g->d_cost);
+        CK(cudaGetLastError());
+        std::vector<float> c(g->nl);
+        CK(cudaMemcpyAsync(c.data(), g->d_cost, 4ull * g->nl, cudaMemcpyDeviceToHost, g->stream));
+        CK(cudaStreamSynchronize(g->stream));
+        g->cost.swap(c);
+    }
+    *out = g->cost.data();
+    return GMK_OK;
+}
+
+// Roots at positions [rb, re) of the cost order of a graph's nl roots
+// (largest cost first, ties by id).
+std::vector<uint32_t> select_roots(uint32_t nl, const float* cost, uint32_t rb, uint32_t re) {
+    std::vector<uint32_t> order(nl);
+    std::iota(order.begin(), order.end(), 0u);
+    std::stable_sort(order.begin(), order.end(),
+                     [cost](uint32_t a, uint32_t b) { return cost[a] > cost[b]; });
+    return std::vector<uint32_t>(order.begin() + rb, order.begin() + re);
+}
+
+// Splits each root into m chunks of its first-level V children in proportion
+// to its cost (m = ceil(cost / unit), at most max_chunks, chunks at least 16
+// children wide) and appends them with per-task cost cost / m and graph
+// index gi.
+void chunk_roots(uint32_t nl, uint32_t n, const std::vector<uint32_t>& roots, const float* cost,
+                 double unit, uint32_t max_chunks, uint32_t gi, std::vector<gmk_task>& out) {
+    const uint32_t nv = n - nl;
+    if (!nv) return;
+    const uint32_t wide = std::max<uint32_t>(1, nv / 16);
+    for (const uint32_t r : roots) {
+        const double c = std::max<double>(cost[r], 0.0);
+        double want = unit > 0 ? std::ceil(c / unit) : 1.0;
+        want = std::max(1.0, std::min(want, (double)std::min(max_chunks, wide)));
+        const uint32_t m = (uint32_t)want;
+        const uint32_t width = (nv + m - 1) / m;
+        for (uint32_t i = 0; i < m; ++i) {
+            const uint64_t first = (uint64_t)nl + (uint64_t)i * width;
+            if (first >= n) break;
+            const uint32_t last = (uint32_t)std::min<uint64_t>(n, first + width);
+            out.push_back(gmk_task{r, (uint32_t)first, last, gi, (float)(c / m)});
+        }
+    }
+}
+
+// Largest cost first (stable), then longest-processing-time assignment to
+// nshards shards (each task to the least-loaded shard, lowest index on ties);
+// keeps the tasks of `shard`.  Every rank computes the same partition from
+// the same costs.
+void order_and_shard(std::vector<gmk_task>& tasks, uint32_t nshards, uint32_t shard) {
+    std::stable_sort(tasks.begin(), tasks.end(),
+                     [](const gmk_task& a, const gmk_task& b) { return a.cost > b.cost; });
+    if (nshards <= 1) return;
+    std::vector<double> load(nshards, 0.0);
+    std::vector<gmk_task> mine;
+    for (const gmk_task& t : tasks) {
+        uint32_t best = 0;
+        for (uint32_t s = 1; s < nshards; ++s)
+            if (load[s] < load[best]) best = s;
+        load[best] += std::max<double>(t.cost, 1e-9);
+        if (best == shard) mine.push_back(t);
+    }
+    tasks.swap(mine);
+}
 
 // One graph of a launch, host side.
 struct GraphJob {
@@ -801,10 +1006,40 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
     if ((rc = grow((void**)&ws.d_arena, &ws.arena_bytes, workers * 4ull * arena_words))) return rc;
     if ((rc = grow((void**)&ws.d_sbuf, &ws.sbuf_bytes, workers * 12ull * smax))) return rc;
 
-    // per graph: root x with chunks of its first-level children
+    // Search tasks.  Planned (the ordered schedule, or a shard of several):
+    // roots split by cost into chunks of their first-level children, largest
+    // first, longest-processing-time partition over the shards.  Otherwise
+    // each graph's roots in id order, every root cut into equal chunks,
+    // chunk-major.
     const size_t ng = jobs.size();
     std::vector<GraphTask> gt(ng);
     std::vector<uint32_t> chunks(ng), cprs(ng);
+    const uint32_t nsh = opts->nshards > 1 ? opts->nshards : 1u;
+    const uint32_t sh = nsh > 1 ? opts->shard : 0u;
+    const bool planned = opts->schedule == GMK_SCHEDULE_ORDERED || nsh > 1 || opts->tasks;
+    std::vector<gmk_task> plan;
+    if (opts->tasks) {
+        // the caller's list, as given (checked by gmk_enumerate)
+        plan.assign(opts->tasks, opts->tasks + opts->n_tasks);
+        for (gmk_task& t : plan) t.graph = 0;
+    } else if (planned) {
+        std::vector<const float*> costs(ng);
+        std::vector<std::vector<uint32_t>> roots(ng);
+        double total = 0;
+        for (size_t i = 0; i < ng; ++i) {
+            const GraphJob& j = jobs[i];
+            costs[i] = j.task_cost;
+            if (!costs[i] && (rc = proxy_costs(j.g, &costs[i]))) return rc;
+            roots[i] = select_roots(j.g->nl, costs[i], j.root_begin, j.root_end);
+            for (const uint32_t r : roots[i]) total += std::max<double>(costs[i][r], 0.0);
+        }
+        const uint32_t max_chunks = opts->schedule == GMK_SCHEDULE_PLAIN ? 1u : 0xFFFFFFFFu;
+        const double unit = total / (double)std::max<uint64_t>(1, 8ull * workers);
+        for (size_t i = 0; i < ng; ++i)
+            chunk_roots(jobs[i].g->nl, jobs[i].g->n, roots[i], costs[i], unit, max_chunks,
+                        (uint32_t)i, plan);
+        order_and_shard(plan, nsh, sh);
+    }
     unsigned long long n_tasks = 0;
     for (size_t i = 0; i < ng; ++i) {
         const GraphJob& j = jobs[i];
@@ -825,18 +1060,6 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
         }
         chunks[i] = chunk;
         cprs[i] = nv ? (nv + chunk - 1) / chunk : 0;
-        const uint32_t* d_order = nullptr;
-        if (opts->schedule == GMK_SCHEDULE_ORDERED && j.task_cost) {
-            std::vector<uint32_t> order(g->nl);
-            std::iota(order.begin(), order.end(), 0u);
-            const float* cost = j.task_cost;
-            std::stable_sort(order.begin(), order.end(),
-                             [cost](uint32_t a, uint32_t b) { return cost[a] > cost[b]; });
-            if ((rc = grow((void**)&g->d_order, &g->order_bytes, 4ull * g->nl))) return rc;
-            CK(cudaMemcpyAsync(g->d_order, order.data(), 4ull * g->nl, cudaMemcpyHostToDevice,
-                               g0->stream));
-            d_order = g->d_order;
-        }
         GraphTask& t = gt[i];
         t.g = gmk::GraphView{g->d_off, g->d_adj, g->n, g->nl};
         t.eh.slots = g->d_eh;
@@ -845,7 +1068,6 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
         t.chunk = chunk;
         t.n_roots = nroots;
         t.root_base = j.root_begin;
-        t.root_order = d_order;
         t.ctr = g->d_ctr;
         t.root_nodes = nullptr;
         if (j.root_nodes) {
@@ -854,11 +1076,26 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
             t.root_nodes = g->d_root_nodes;
         }
         t.task_begin = n_tasks;
-        n_tasks += (unsigned long long)nroots * cprs[i];
+        if (!planned) n_tasks += (unsigned long long)nroots * cprs[i];
         CK(cudaMemsetAsync(g->d_ctr, 0, sizeof(Counters), g0->stream));
     }
-    const uint32_t nsh = opts->nshards ? opts->nshards : 1u, sh = opts->nshards ? opts->shard : 0u;
-    const unsigned long long my_tasks = n_tasks > sh ? (n_tasks - sh + nsh - 1) / nsh : 0;
+    const TaskEntry* d_tasks = nullptr;
+    if (planned) {
+        n_tasks = plan.size();
+        std::vector<TaskEntry> tab(plan.size());
+        for (size_t i = 0; i < plan.size(); ++i)
+            tab[i] = TaskEntry{plan[i].root, plan[i].first, plan[i].last, plan[i].graph};
+        if (!tab.empty()) {
+            if ((rc = grow((void**)&g0->d_tasks, &g0->tasks_bytes, sizeof(TaskEntry) * tab.size())))
+                return rc;
+            CK(cudaMemcpyAsync(g0->d_tasks, tab.data(), sizeof(TaskEntry) * tab.size(),
+                               cudaMemcpyHostToDevice, g0->stream));
+            // the table is read by the launch: the host copy must outlive the copy
+            CK(cudaStreamSynchronize(g0->stream));
+            d_tasks = g0->d_tasks;
+        }
+    }
+    const unsigned long long my_tasks = n_tasks;
     if ((rc = grow((void**)&ws.d_graphs, &ws.graphs_bytes, sizeof(GraphTask) * ng))) return rc;
     CK(cudaMemcpyAsync(ws.d_graphs, gt.data(), sizeof(GraphTask) * ng, cudaMemcpyHostToDevice,
                        g0->stream));
@@ -888,11 +1125,23 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
                 return rc;
         }
     }
+    // in-launch work sharing (count-only warp runs that split: batched / ordered)
+    const bool share = warp && split_min && !opts->emit && !opts->no_sharing;
+    unsigned long long dq_word_cap = 0, dq_idx_cap = 0;
+    if (share) {
+        dq_word_cap = std::max<unsigned long long>(1ull << 22, workers * 4096ull);
+        dq_idx_cap = std::max<unsigned long long>(1ull << 16, workers * 64ull);
+        const size_t had = ws.dq_idx_bytes;
+        const void* had_p = ws.d_dq_idx;
+        if ((rc = grow((void**)&ws.d_dq_words, &ws.dq_words_bytes, dq_word_cap * 4))) return rc;
+        if ((rc = grow((void**)&ws.d_dq_idx, &ws.dq_idx_bytes, dq_idx_cap * 8))) return rc;
+        if (ws.dq_idx_bytes != had || ws.d_dq_idx != had_p) ws.dq_dirty = ws.dq_idx_bytes / 8;
+    }
     const unsigned grid = (unsigned)(threads / block);
     const unsigned long long watchdog_ns = (unsigned long long)opts->watchdog_ms * 1000000ull;
     const uint32_t pair_limit = opts->pair_limit ? opts->pair_limit : kDefaultPairLimit;
     Counters h;          // launch-wide flags (graph 0's counters)
-    unsigned long long tasks_total = 0, tasks_done = 0;
+    unsigned long long tasks_total = 0, tasks_done = 0, donations = 0;
     uint32_t rounds = 0;
     int warp_emit_rc = GMK_OK;
     CK(cudaEventRecord(g0->ev0, g0->stream));
@@ -900,8 +1149,8 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
         const GraphJob& j = jobs[0];
         enumerate_kernel<<<grid, kBlock, 0, g0->stream>>>(
             gt[0].g, j.k, g0->d_ctr, ws.d_arena, arena_words, ws.d_sbuf, smax, pair_limit, n_tasks,
-            chunks[0], cprs[0], gt[0].root_order, j.root_begin, opts->result_limit,
-            opts->emit ? ws.d_out : nullptr, out_words, watchdog_ns, sh, nsh);
+            chunks[0], cprs[0], d_tasks, j.root_begin, opts->result_limit,
+            opts->emit ? ws.d_out : nullptr, out_words, watchdog_ns);
         CK(cudaGetLastError());
         CK(cudaEventRecord(g0->ev1, g0->stream));
         CK(cudaMemcpyAsync(&h, g0->d_ctr, sizeof(h), cudaMemcpyDeviceToHost, g0->stream));
@@ -926,8 +1175,24 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
         a.out_buf = opts->emit ? ws.d_out : nullptr;
         a.out_cap = out_words;
         a.watchdog_ns = watchdog_ns;
-        a.shard = sh;
-        a.nshards = nsh;
+        a.tasks = d_tasks;
+        std::memset(&a.share, 0, sizeof(a.share));
+        if (share) {
+            RoundCounters* rcd = g0->d_rc;
+            a.share.words = ws.d_dq_words;
+            a.share.word_cap = dq_word_cap;
+            a.share.idx = ws.d_dq_idx;
+            a.share.idx_cap = dq_idx_cap;
+            a.share.used = &rcd->dq_used;
+            a.share.tail = &rcd->dq_tail;
+            a.share.head = &rcd->dq_head;
+            a.share.outstanding = &rcd->outstanding;
+            a.share.beat = &rcd->beat;
+            a.share.donated = &rcd->donated;
+            a.share.idle = &rcd->idle;
+            a.share.full = &rcd->dq_full;
+            a.share.min_nodes = opts->donate_min_nodes ? opts->donate_min_nodes : kDefaultDonateMin;
+        }
         // Record mode streams: each round writes one of two record buffers,
         // and while the next round runs the host hands the previous round's
         // records to the sink.  A round winds down (splits its tasks into the
@@ -956,6 +1221,11 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
             a.out_buf = opts->emit ? outb[round & 1] : nullptr;
             CK(cudaMemsetAsync(g0->d_rc, 0, sizeof(RoundCounters), g0->stream));
             CK(cudaMemsetAsync(&g0->d_rc->out_fail, 0xFF, 2 * sizeof(unsigned long long), g0->stream));
+            if (share && ws.dq_dirty) {
+                CK(cudaMemsetAsync(ws.d_dq_idx, 0, 8ull * std::min<unsigned long long>(ws.dq_dirty, dq_idx_cap),
+                                   g0->stream));
+                ws.dq_dirty = 0;
+            }
             // k >= 2: the instantiation with filter bitmaps for long lists
             // (at k = 1 their code alone cost 15 %, so it is a separate kernel)
             const bool bits = a.single.k >= 2;
@@ -981,6 +1251,10 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
             ++rounds;
             tasks_total += a.queue_len;
             tasks_done += std::min<unsigned long long>(r.tasks_done, a.queue_len);
+            if (share) {
+                ws.dq_dirty = std::max<unsigned long long>(ws.dq_dirty, std::min(r.dq_tail, dq_idx_cap));
+                donations += r.donated;
+            }
             if (opts->emit) {
                 // records end where the first one found no room
                 pending = round & 1;
@@ -1037,6 +1311,7 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
         out->truncated = opts->result_limit && hc.count >= opts->result_limit;
         out->threads = (uint32_t)threads;
         out->rounds = rounds;
+        out->donations = donations;
     }
     switch (h.error) {
         case gmk::TASK_OK: break;
@@ -1079,6 +1354,34 @@ int check_opts(const gmk_opts* opts) {
 
 extern "C" {
 
+int gmk_plan_tasks(uint32_t n, uint32_t n_left, const float* root_cost, uint32_t root_begin,
+                   uint32_t root_end, uint64_t target_tasks, uint32_t max_chunks,
+                   uint32_t nshards, uint32_t shard, gmk_task* out, uint64_t* n_out) {
+    if (!n_out || n_left > n || (!root_cost && n_left) || root_begin > root_end ||
+        root_end > n_left || (nshards > 1 && shard >= nshards))
+        return GMK_E_INVAL;
+    std::vector<uint32_t> roots = select_roots(n_left, root_cost, root_begin, root_end);
+    double total = 0;
+    for (const uint32_t r : roots) total += std::max<double>(root_cost[r], 0.0);
+    std::vector<gmk_task> plan;
+    chunk_roots(n_left, n, roots, root_cost, total / (double)std::max<uint64_t>(1, target_tasks),
+                max_chunks ? max_chunks : 0xFFFFFFFFu, 0, plan);
+    order_and_shard(plan, nshards, shard);
+    if (out) std::copy(plan.begin(), plan.end(), out);
+    *n_out = plan.size();
+    return GMK_OK;
+}
+
+int gmk_root_costs(gmk_graph* g, float* out) {
+    if (!g || !out) return GMK_E_INVAL;
+    CK(cudaSetDevice(g->device));
+    if (g->nl == 0) return GMK_OK;
+    const float* c = nullptr;
+    if (int rc = proxy_costs(g, &c)) return rc;
+    std::copy(c, c + g->nl, out);
+    return GMK_OK;
+}
+
 int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user, gmk_stats* out) {
     if (!g || !opts || !out) return GMK_E_INVAL;
     if (int rc = check_opts(opts)) return rc;
@@ -1087,6 +1390,14 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
     if (opts->root_nodes && opts->engine != GMK_ENGINE_WARP) return GMK_E_INVAL;
     const uint32_t root_end = opts->root_end ? opts->root_end : g->nl;
     if (root_end > g->nl || opts->root_begin > root_end) return GMK_E_INVAL;
+    if (opts->tasks) {
+        if (opts->nshards > 1 || opts->root_begin || opts->root_end) return GMK_E_INVAL;
+        for (uint64_t i = 0; i < opts->n_tasks; ++i) {
+            const gmk_task& t = opts->tasks[i];
+            if (t.root >= g->nl || t.first < g->nl || t.first >= t.last || t.last > g->n)
+                return GMK_E_INVAL;
+        }
+    }
     std::memset(out, 0, sizeof(*out));
     CK(cudaSetDevice(g->device));
     if (g->nl == 0 || g->n == g->nl || opts->root_begin == root_end) return GMK_OK;   // nothing to do
@@ -1100,7 +1411,7 @@ int gmk_enumerate_batch(gmk_graph* const* graphs, uint32_t n_graphs, const uint3
     if (!graphs || !opts || !outs || n_graphs == 0) return GMK_E_INVAL;
     if (int rc = check_opts(opts)) return rc;
     if (opts->engine != GMK_ENGINE_WARP || opts->emit || opts->result_limit || opts->root_nodes ||
-        opts->root_begin || opts->root_end || (opts->nshards > 1))
+        opts->root_begin || opts->root_end || (opts->nshards > 1) || opts->tasks)
         return GMK_E_INVAL;
     std::memset(outs, 0, sizeof(gmk_stats) * n_graphs);
     std::vector<GraphJob> jobs;
@@ -1416,7 +1727,7 @@ int gmk_enumerate_noalloc(const uint32_t* d_offsets, const uint32_t* d_adj, uint
     gmk::GraphView gv{d_offsets, d_adj, n, n_left};
     enumerate_kernel<<<threads / kBlock, kBlock, 0, s>>>(
         gv, k, ctr, arenas, arena_words, sbuf, max_members, kDefaultPairLimit, n_tasks, chunk,
-        chunks_per_root, nullptr, 0u, result_limit, nullptr, 0ull, 0ull, 0u, 1u);
+        chunks_per_root, nullptr, 0u, result_limit, nullptr, 0ull, 0ull);
     CK(cudaGetLastError());
     Counters h;
     CK(cudaMemcpyAsync(&h, ctr, sizeof(h), cudaMemcpyDeviceToHost, s));
@@ -1510,7 +1821,7 @@ uint64_t order_hash(const gmk_graph* g, const gmk_opts* o) {
 int gmk_enumerate_resumable(gmk_graph* g, const gmk_opts* opts, const char* checkpoint_path,
                             uint32_t batch_roots, uint32_t max_batches, gmk_sink sink,
                             void* user, gmk_stats* out) {
-    if (!g || !opts || !out || !checkpoint_path) return GMK_E_INVAL;
+    if (!g || !opts || !out || !checkpoint_path || opts->tasks) return GMK_E_INVAL;
     std::memset(out, 0, sizeof(*out));
     Checkpoint c;
     bool exists = false;
@@ -1562,6 +1873,7 @@ int gmk_enumerate_resumable(gmk_graph* g, const gmk_opts* opts, const char* chec
         out->tasks += st.tasks;
         out->tasks_done += st.tasks_done;
         out->rounds += st.rounds;
+        out->donations += st.donations;
         out->threads = st.threads;
         ++batches;
         if (!write_checkpoint(checkpoint_path, c)) return GMK_E_IO;

@@ -19,7 +19,7 @@
 extern "C" {
 #endif
 
-#define GMK_ABI_VERSION 2
+#define GMK_ABI_VERSION 3
 
 enum {
     GMK_OK = 0,
@@ -73,7 +73,9 @@ enum {
     GMK_SCHEDULE_PLAIN = 0,    /* one task per root, roots in id order, no splitting */
     GMK_SCHEDULE_BATCHED = 1,  /* roots split into chunks, persistent work queue; unfinished
                                   search trees are split into the next round's tasks */
-    GMK_SCHEDULE_ORDERED = 2   /* batched, roots ordered by a caller-given cost (largest first) */
+    GMK_SCHEDULE_ORDERED = 2   /* batched over planned tasks: roots split into chunks in
+                                  proportion to a caller-given cost (task_cost, e.g. the
+                                  subtree-size model's prediction), largest first */
 };
 
 /* Search engines (same rules, same result set). */
@@ -98,8 +100,9 @@ typedef struct {
     const float* task_cost;   /* GMK_SCHEDULE_ORDERED: one cost per root U vertex (n_left) */
     uint32_t pair_limit;      /* node rules (shortcut, forcing, exclusion prune) run while
                                  (|S|+|C_U|)*(|S|+|C_V|) <= pair_limit; 0 = 4096 */
-    uint32_t shard, nshards;  /* run only tasks t with t % nshards == shard (one GPU of
-                                 several); nshards 0 or 1 = all tasks */
+    uint32_t shard, nshards;  /* one GPU of several: run only this shard's tasks of the
+                                 longest-processing-time partition of gmk_plan_tasks (costs:
+                                 task_cost, else gmk_root_costs); nshards 0 or 1 = all */
     int32_t engine;           /* GMK_ENGINE_* */
     uint32_t split_min_nodes; /* warp engine, batched/ordered: a task is split only after this
                                  many nodes; 0 = 64 */
@@ -110,6 +113,17 @@ typedef struct {
     uint64_t* root_nodes;     /* optional, warp engine: host array of n_left counters; the
                                  search nodes of each root's tasks are added to its entry
                                  (the subtree sizes the learned schedule trains on) */
+    uint32_t donate_min_nodes; /* warp engine, batched/ordered, emit = 0: in-launch work
+                                 sharing -- a busy task that has run this many nodes gives the
+                                 shallowest unexplored part of its tree to an idle warp;
+                                 0 = 16 */
+    int32_t no_sharing;       /* 1: no in-launch sharing (unfinished trees only split into the
+                                 next launch, as emit = 1 runs do) */
+    const struct gmk_task_* tasks; /* optional explicit task list (gmk_task, e.g. from
+                                 gmk_plan_tasks): run exactly these tasks in this order,
+                                 instead of planning; needs nshards <= 1, no root range,
+                                 and one graph.  Used to re-run a failed rank's shard. */
+    uint64_t n_tasks;         /* entries of tasks */
 } gmk_opts;
 
 typedef struct {
@@ -129,6 +143,7 @@ typedef struct {
     int32_t truncated;        /* 1 if result_limit stopped the search */
     uint32_t threads;         /* search threads used */
     uint32_t rounds;          /* kernel launches (rounds of split tasks) */
+    uint64_t donations;       /* search-tree pieces handed to idle warps inside launches */
 } gmk_stats;
 
 /* Called from the calling thread after the kernel finished, once per result;
@@ -244,6 +259,36 @@ int gmk_mlp_gradient(gmk_mlp* m, const float* x, const float* y, uint32_t n, flo
 int gmk_mlp_train(gmk_mlp* m, const float* x, const float* y, uint32_t n, uint32_t epochs,
                   float lr, float* loss);
 int gmk_mlp_predict(gmk_mlp* m, const float* x, uint32_t n, float* out);
+
+/* ---- task planning (no counterpart in the reference, whose host loop takes the
+ * top-level vertices one at a time in id order, src/main.cu:1078-1111) */
+
+/* One search task: root x (a U vertex) with the first-level V children
+ * [first, last) of its search -- the maximal k-biplexes whose smallest U
+ * vertex is x and whose smallest V vertex lies in [first, last). */
+typedef struct gmk_task_ {
+    uint32_t root, first, last;
+    uint32_t graph;           /* index of the graph in a batch (0 for one graph) */
+    float cost;               /* predicted cost of the task */
+} gmk_task;
+
+/* Cost proxy of every root task (n_left floats): 1 + sum over the root's
+ * neighbours y of |N(y) above x| -- the U vertices that can join x through a
+ * common neighbour.  Computed on the graph's device once and cached. */
+int gmk_root_costs(gmk_graph* g, float* out);
+
+/* Host-only planner, the one the ordered schedule and sharding use.  The roots
+ * at positions [root_begin, root_end) of the cost order (largest first, ties
+ * by id) are each split into ceil(cost / unit) chunks of their first-level V
+ * children (unit = total cost / target_tasks; at most max_chunks per root,
+ * chunks at least 16 children wide), ordered by per-task cost (largest first)
+ * and, with nshards > 1, assigned to shards by longest processing time (each
+ * task to the least-loaded shard, lowest index on ties).  Writes this shard's
+ * tasks to out (NULL: count only) and their number to *n_out; out must hold
+ * *n_out entries from a counting call with the same arguments. */
+int gmk_plan_tasks(uint32_t n, uint32_t n_left, const float* root_cost, uint32_t root_begin,
+                   uint32_t root_end, uint64_t target_tasks, uint32_t max_chunks,
+                   uint32_t nshards, uint32_t shard, gmk_task* out, uint64_t* n_out);
 
 /* No counterpart in the reference.  Canonical per-result hash pair (the set
  * summary's h1/h2): ids are the global ids of X u Y in any order, nx = |X|,

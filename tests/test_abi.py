@@ -36,7 +36,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_strerror():
     lib = G.load_library()
-    assert lib.gmk_abi_version() == 2
+    assert lib.gmk_abi_version() == 3
     for code in list(range(0, -13, -1)) + [1]:
         assert lib.gmk_strerror(code).decode() != "unknown error"
 

@@ -1496,6 +1496,7 @@ __device__ __forceinline__ bool donate_top(Ctx& t, const Donation& db, uint32_t 
     for (uint32_t i = t.lane; i < 2 * c0; i += 32) lr[i] = a0[i];
     #pragma unroll 1
     for (uint32_t i = t.lane; i < 2 * c1; i += 32) lr[2 * c0 + i] = a1[i];
+    __threadfence();                       // every lane's record words before the slot
     __syncwarp();
     if (t.lane == 0) {
         atomicAdd(db.outstanding, 1ull);   // before the record can be taken and finished

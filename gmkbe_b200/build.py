@@ -1,6 +1,6 @@
 """Build the in-tree native artefacts.
 
-    python -m gmkbe_b200.build          # libgmk.so + the gmk CLI (sm_100a)
+    python -m gmkbe_b200.build          # libgmk.so + the gmk CLI (sm_100a), gmk-convert
 
 Everything is compiled with nvcc for sm_100a only and written next to the
 sources (gmkbe_b200/libgmk.so, gmkbe_b200/gmk), so the built files travel with
@@ -21,6 +21,8 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-I" + os.path.join(ROOT, "include")
 
 LIB = os.path.join(PKG, "libgmk.so")
 CLI = os.path.join(PKG, "gmk")
+CONVERT = os.path.join(PKG, "gmk-convert")
+CXX = os.environ.get("CXX", "g++")
 
 
 def _run(cmd: list[str]) -> None:
@@ -43,6 +45,9 @@ def build(force: bool = False) -> None:
     if force or _stale(CLI, deps + [LIB]):
         _run([NVCC, *ARCH, *COMMON, "-o", CLI, os.path.join(CSRC, "gmk_cli.cpp"),
               "-L" + PKG, "-lgmk", "-Xlinker", "-rpath=$ORIGIN"])
+    conv_src = os.path.join(CSRC, "gmk_convert.cpp")
+    if force or _stale(CONVERT, [conv_src]):
+        _run([CXX, "-O3", "-std=c++17", "-pthread", "-o", CONVERT, conv_src])
 
 
 if __name__ == "__main__":

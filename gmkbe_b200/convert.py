@@ -1,6 +1,7 @@
 """Edge list -> `.graph.bin`, with the ordering of the reference's converter.
 
-    python -m gmkbe_b200.convert -i edges.txt -o out[.graph.bin]
+    python -m gmkbe_b200.convert -i edges.txt -o out[.graph.bin]   # gmk-convert, threaded
+    gmkbe_b200/gmk-convert -i edges.txt -o out [--threads N]        # the same, directly
 
 Reads text lines "u v ..." (lines starting with % or # are comments; a size
 header line such as KONECT's must be removed first, as for the reference's
@@ -15,7 +16,9 @@ deg-1 (right) in wrapping 32-bit arithmetic (gmkbe_b200.graphgen.relabel).
 from __future__ import annotations
 
 import argparse
+import os
 import re
+import subprocess
 import sys
 
 import numpy as np
@@ -55,6 +58,22 @@ def parse_edge_list(data: bytes) -> tuple[np.ndarray, np.ndarray]:
     return np.asarray(us, dtype=np.int64), np.asarray(vs, dtype=np.int64)
 
 
+NATIVE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "gmk-convert")
+
+
+def convert_native(infile: str, outfile: str, threads: int = 0, min_chunk: int = 0) -> str:
+    """The multi-threaded C++ converter (gmk-convert, built by gmkbe_b200.build);
+    same output as convert().  Returns the output path."""
+    if not os.path.exists(NATIVE):
+        raise FileNotFoundError(f"{NATIVE} not built; run `python -m gmkbe_b200.build`")
+    cmd = [NATIVE, "-i", infile, "-o", outfile]
+    if threads:
+        cmd += ["--threads", str(threads)]
+    if min_chunk:
+        cmd += ["--min-chunk", str(min_chunk)]
+    return subprocess.run(cmd, check=True, capture_output=True, text=True).stdout.strip()
+
+
 def convert(infile: str, outfile: str) -> str:
     """Writes the `.graph.bin` of an edge-list file; returns the output path."""
     if not outfile.endswith(".graph.bin"):
@@ -69,8 +88,9 @@ def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("-i", required=True, help="edge list")
     ap.add_argument("-o", required=True, help="output prefix or .graph.bin path")
+    ap.add_argument("--python", action="store_true", help="the single-threaded numpy port")
     a = ap.parse_args(argv)
-    print(convert(a.i, a.o))
+    print(convert(a.i, a.o) if a.python or not os.path.exists(NATIVE) else convert_native(a.i, a.o))
     return 0
 
 

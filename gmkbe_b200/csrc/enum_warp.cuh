@@ -41,6 +41,8 @@ constexpr uint32_t kSrcCap = 17;          // k + 1 sources, k <= 16
 constexpr uint32_t FL_ROOT = 16u;         // frame flag: the task's root frame
 constexpr uint32_t FL_BITS0 = 32u;        // frame flags: filter bitmaps of list 0 / list 1
 constexpr uint32_t FL_BITS1 = 64u;        //   follow the frame's lists (add_filter_bits)
+constexpr uint32_t FL_ONE_PHASE = 128u;   // frame flag: iterate the current phase only (a
+                                          //   donated range of its first side's children)
 constexpr uint32_t kBitsMinList = 64;     // shorter lists filter their children by probing
 constexpr uint32_t kBitsMaxZ = 8;         // bitmaps for at most this many members
 constexpr unsigned long long kEmptyKey = ~0ull;
@@ -1238,10 +1240,12 @@ __device__ bool next_child(Ctx& t, uint32_t cur, ChildReq* req) {
         const bool opp_done = phase == 1;
         uint32_t c = 0, p = kNoPos;
         bool have = false;
+        // F_END bounds the current phase's positions: a root chunk's last
+        // V child, or the end of a donated range of children
         if (h.flags & gbit(s)) {
-            const uint32_t end = phase == 0 && h.end < side_end(g, s) ? h.end : side_end(g, s);
+            const uint32_t end = h.end < side_end(g, s) ? h.end : side_end(g, s);
             if (pos < end) { c = pos; p = kNoPos; ++pos; have = true; }
-        } else if (pos < h.cnt.get(s)) {
+        } else if (pos < (h.end < h.cnt.get(s) ? h.end : h.cnt.get(s))) {
             p = pos;
             c = t.arena[h.off.get(s) + 2 * p];
             ++pos;
@@ -1257,6 +1261,7 @@ __device__ bool next_child(Ctx& t, uint32_t cur, ChildReq* req) {
         if (!have) {
             if (phase == 2) break;
             ++phase;
+            if (phase == 1 && (h.flags & FL_ONE_PHASE)) phase = 2;
             if (phase == 1) {
                 const int s2 = 1 - (int)h.order;
                 pos = (h.flags & gbit(s2)) ? h.lo.get(s2) + 1 : 0;
@@ -1390,16 +1395,18 @@ __device__ bool split_path(Ctx& t, const SplitBuf& sb, uint32_t cur) {
 
 // ----------------------------------------------------------------- work sharing
 
-// In-launch work sharing.  A warp that runs out of tasks registers as idle;
-// a busy warp that sees idle warps (at its poll points) donates the shallowest
-// frame of its path that still has unexplored children -- the largest piece of
-// its remaining tree -- as a record in the same format as split_path's, and
-// marks that frame finished in its own stack.  Idle warps take records in
-// order.  `outstanding` counts the launch's unfinished tasks (the queue's
-// entries plus the donations, minus the finished), kept offset by the queue
-// length: the launch's work is done when it returns to -queue_len.  Records
-// live in a bump-allocated buffer for the launch; once it is full, donation
-// stops and the busy warps split into the next round as before.
+// In-launch work sharing.  A warp that runs out of tasks takes a ticket t (a
+// counter) and waits on slot t of the record index.  A busy warp that sees
+// more tickets than reserved slots (at its poll points) splits the shallowest
+// frame of its path that still has unexplored children: the first half of
+// that frame's remaining children in the current phase goes into a record
+// (F_POS .. F_END, one phase only), the warp keeps the rest.  So the work
+// spreads by halving, and each waiting warp watches its own slot -- no retry
+// loops on shared counters.  `outstanding` counts the launch's unfinished
+// tasks (the queue's entries plus the donations, minus the finished), offset
+// by the queue length: the launch's work is done when it is -queue_len.
+// Records live in a bump-allocated buffer for the launch; once it is full,
+// donation stops and busy warps split into the next round as before.
 struct Donation {
     uint32_t* words;
     unsigned long long word_cap;
@@ -1407,43 +1414,55 @@ struct Donation {
     unsigned long long idx_cap;
     unsigned long long* used;         // words reserved
     unsigned long long* tail;         // slots reserved
-    unsigned long long* head;         // slots taken
+    unsigned long long* claim;        // tickets taken by waiting warps
     unsigned long long* outstanding;  // unfinished tasks - queue_len (mod 2^64)
-    unsigned long long* beat;         // busy warps' heartbeat while others wait
     unsigned long long* donated;      // records published (statistics)
-    unsigned int* idle;               // warps waiting for a record
     int* full;                        // a reservation failed: no more donations
     uint32_t min_nodes;               // a task donates only after this many nodes
 };
 
-// Is there anything left to iterate in entered frame f (phase < 2)?  Exact
-// for the sides' positions; the "U child needs a V member" rule of phase 1 is
-// left to the taker (it then finds nothing).
-__device__ __forceinline__ bool frame_has_more(const GraphView& g, const uint32_t* f) {
+// Positions left in the current phase of entered frame f ([pos, lim)), and
+// whether a second phase follows.
+struct Rest {
+    uint32_t pos, lim;
+    bool next_phase;
+};
+
+__device__ __forceinline__ Rest frame_rest(const GraphView& g, const uint32_t* f) {
+    Rest r{0, 0, false};
     const uint32_t phase = f[F_PHASE];
-    if (phase >= 2) return false;
+    if (phase >= 2) return r;
     const uint32_t order = f[F_ORDER];
     const int s = phase == 0 ? (int)order : 1 - (int)order;
-    const bool gl = f[F_FLAGS] & (s ? FL_G1 : FL_G0);
-    const uint32_t limit = gl ? (phase == 0 && f[F_END] < side_end(g, s) ? f[F_END] : side_end(g, s))
-                              : f[F_CNT0 + s];
-    if (f[F_POS] < limit) return true;
-    if (phase == 1) return false;
-    const int s2 = 1 - s;
-    if (f[F_FLAGS] & (s2 ? FL_G1 : FL_G0)) return f[F_LO0 + s2] + 1 < side_end(g, s2);
-    return f[F_CNT0 + s2] > 0;
+    const uint32_t flags = f[F_FLAGS];
+    const uint32_t side = (flags & (s ? FL_G1 : FL_G0)) ? side_end(g, s) : f[F_CNT0 + s];
+    r.pos = f[F_POS];
+    r.lim = f[F_END] < side ? f[F_END] : side;
+    if (r.pos > r.lim) r.pos = r.lim;
+    if (phase == 0 && !(flags & FL_ONE_PHASE)) {
+        const int s2 = 1 - s;
+        r.next_phase = (flags & (s2 ? FL_G1 : FL_G0)) ? f[F_LO0 + s2] + 1 < side_end(g, s2)
+                                                      : f[F_CNT0 + s2] > 0;
+    }
+    return r;
 }
 
-// Donates the shallowest pending frame above or at `cur` (entered frames
-// only).  Returns true when a record was published.  Inlined: an out-of-line
-// call makes the search loop save its live registers around the call site
-// (ptxas: 48 -> 270 bytes of stack and 5x the spill loads).
+// Donates part of the shallowest entered frame above or at `cur` that has
+// work left: half of its current phase's remaining children (the first
+// half), or the one child left, or -- when the current phase is used up --
+// the whole second phase.  Returns true when a record was published.
+// Inlined: an out-of-line call makes the search loop save its live
+// registers around the call site (ptxas: 48 -> 270 bytes of stack and 5x
+// the spill loads).
 __device__ __forceinline__ bool donate_top(Ctx& t, const Donation& db, uint32_t cur) {
     uint32_t best = kNoPos;
+    Rest rb{0, 0, false};
     #pragma unroll 1
     for (uint32_t x = cur; x != kNoPos; x = t.arena[x + F_PARENT_SLOT]) {
         const uint32_t* f = t.arena + x;
-        if ((f[F_FLAGS] & FL_ENTERED) && frame_has_more(t.g, f)) best = x;
+        if (!(f[F_FLAGS] & FL_ENTERED)) continue;
+        const Rest r = frame_rest(t.g, f);
+        if (r.lim > r.pos || r.next_phase) { best = x; rb = r; }
     }
     if (best == kNoPos) return false;
     const uint32_t* f = t.arena + best;
@@ -1464,6 +1483,23 @@ __device__ __forceinline__ bool donate_top(Ctx& t, const Donation& db, uint32_t 
     if (!bcast(ok)) return false;
     w0 = bcast(w0);
     slot = bcast(slot);
+    // the split: record phase / range, and what the donor keeps
+    const uint32_t rem = rb.lim - rb.pos;
+    uint32_t r_phase = f[F_PHASE], r_pos = rb.pos, r_end, r_flags = f[F_FLAGS];
+    uint32_t keep_phase = f[F_PHASE], keep_pos;
+    if (rem >= 1) {
+        r_end = rb.pos + (rem >= 2 ? rem / 2 : 1u);
+        r_flags |= FL_ONE_PHASE;
+        keep_pos = r_end;
+    } else {
+        // the current phase is used up: the record takes the second phase
+        const int s2 = f[F_ORDER] ? 0 : 1;
+        r_phase = 1;
+        r_pos = (f[F_FLAGS] & (s2 ? FL_G1 : FL_G0)) ? f[F_LO0 + s2] + 1 : 0u;
+        r_end = 0xFFFFFFFFu;
+        keep_phase = 2;
+        keep_pos = f[F_POS];
+    }
     uint32_t* r = db.words + w0;
     if (t.lane == 0) { r[0] = ns; r[1] = c0; r[2] = c1; r[3] = t.gid; }
     uint32_t* rs = r + kRecHeader;
@@ -1488,7 +1524,14 @@ __device__ __forceinline__ bool donate_top(Ctx& t, const Donation& db, uint32_t 
         rs[ns + i] = miss;
     }
     uint32_t* fr = rs + 2 * ns;
-    if (t.lane < F_WORDS) fr[t.lane] = f[t.lane];
+    if (t.lane < F_WORDS) {
+        uint32_t v = f[t.lane];
+        v = t.lane == F_PHASE ? r_phase : v;
+        v = t.lane == F_POS ? r_pos : v;
+        v = t.lane == F_END ? r_end : v;
+        v = t.lane == F_FLAGS ? r_flags : v;
+        fr[t.lane] = v;
+    }
     uint32_t* lr = fr + F_WORDS;
     const uint32_t* a0 = t.arena + f[F_OFF0];
     const uint32_t* a1 = t.arena + f[F_OFF1];
@@ -1503,7 +1546,8 @@ __device__ __forceinline__ bool donate_top(Ctx& t, const Donation& db, uint32_t 
         atomicAdd(db.donated, 1ull);
         __threadfence();
         atomicExch(db.idx + slot, w0 + 1);
-        t.arena[best + F_PHASE] = 2;       // the rest of this frame is the record's now
+        t.arena[best + F_PHASE] = keep_phase;   // the donor keeps the rest
+        t.arena[best + F_POS] = keep_pos;
     }
     __syncwarp();
     return true;
@@ -1549,14 +1593,11 @@ __device__ __forceinline__ unsigned long long run_dfs(Ctx& t, const Outputs& o, 
                 // in-launch sharing while its buffer has room; splitting into
                 // the next round otherwise
                 const bool share = !kRec && db && !load_flag(db->full);
-                if (share) {
-                    const unsigned idle = *(volatile const unsigned*)db->idle;
-                    if (idle) {
-                        atomicAdd(db->beat, 1ull);
-                        const unsigned long long avail = *(volatile const unsigned long long*)db->tail -
-                                                         *(volatile const unsigned long long*)db->head;
-                        give = task_nodes >= db->min_nodes && avail < idle;
-                    }
+                if (share && task_nodes >= db->min_nodes) {
+                    // waiting warps without a record: tickets beyond the reserved slots
+                    const long long want = (long long)(*(volatile const unsigned long long*)db->claim -
+                                                       *(volatile const unsigned long long*)db->tail);
+                    give = want > 0;
                 }
                 hungry = may_split && task_nodes >= 1 &&
                          ((!share && lim.split_min_nodes && task_nodes >= lim.split_min_nodes &&

@@ -57,10 +57,13 @@ struct RoundCounters {
     unsigned long long next_fail;   // lowest split-record index that found no room (~0: none)
     int split_refused;              // first reason a split was refused (0 = none)
     int pad;
-    // in-launch work sharing (gmk::warp::Donation)
-    unsigned long long dq_used, dq_tail, dq_head, outstanding, beat, donated;
-    unsigned int idle;
-    int dq_full;
+    // in-launch work sharing (gmk::warp::Donation); the polled counters sit on
+    // their own 128-byte lines
+    unsigned long long dq_used, donated;
+    int dq_full, pad2;
+    alignas(128) unsigned long long dq_tail;
+    alignas(128) unsigned long long dq_claim;
+    alignas(128) unsigned long long outstanding;
 };
 
 constexpr int kBlock = 128;
@@ -193,12 +196,10 @@ struct WarpArgs {
     gmk::warp::Donation share;         // in-launch work sharing (share.words null: off)
 };
 
-// An idle warp gives up when no busy warp has shown a sign of life (a
-// heartbeat at its poll points) for this long: a safety net that turns a
-// lost task into an error instead of a kernel that never ends.
+// A waiting warp gives up when the launch's remaining work shows no change
+// (no task finished, no record reserved) for this long: a safety net that
+// turns a lost task into an error instead of a kernel that never ends.
 constexpr unsigned long long kIdleLimitNs = 10ull * 1000000000ull;
-// Longest wait for a reserved record to be published by its writer.
-constexpr unsigned long long kPublishLimitNs = 1000000000ull;
 
 // Points the warp's context and counters at graph gid of the launch.  A
 // one-graph launch reads its graph from the kernel parameters, so the values
@@ -288,76 +289,66 @@ enumerate_warp_kernel(const __grid_constant__ WarpArgs a) {
         stop = bcast(stop);
         j = bcast(j);
         if (stop) break;
+        const uint32_t* rec = nullptr;
         if (j >= a.queue_len) {
-            // the queue is empty: wait for a donated record, or for the end
-            // of the launch's work (no task outstanding)
+            // the queue is empty: take a ticket and wait for its slot's
+            // donated record, or for the end of the launch's work (no task
+            // outstanding)
             if (!db) break;
-            unsigned long long slot = ~0ull, w = 0;
+            unsigned long long w = 0;
             int quit = 0;
             if (lane == 0) {
-                atomicAdd(db->idle, 1u);
-                unsigned long long last_beat = *(volatile unsigned long long*)db->beat;
-                unsigned long long t_beat = gmk::now_ns();
-                unsigned sleep_ns = 32;
-                for (;;) {
-                    if (gmk::load_flag(o.stop)) { quit = 1; break; }
-                    const unsigned long long h = *(volatile unsigned long long*)db->head;
-                    const unsigned long long tl = *(volatile unsigned long long*)db->tail;
-                    if (h < (tl < db->idx_cap ? tl : db->idx_cap)) {
-                        if (atomicCAS(db->head, h, h + 1) == h) { slot = h; break; }
-                        continue;
-                    }
-                    if (*(volatile unsigned long long*)db->outstanding + a.queue_len == 0) {
-                        quit = 1;
-                        break;
-                    }
-                    const unsigned long long b = *(volatile unsigned long long*)db->beat;
-                    const unsigned long long now = gmk::now_ns();
-                    if (b != last_beat) {
-                        last_beat = b;
-                        t_beat = now;
-                    } else if (now - t_beat > kIdleLimitNs) {
-                        atomicCAS(o.error, 0, gmk::TASK_E_TIMEOUT);
-                        atomicExch(o.stop, 1);
-                        quit = 1;
-                        break;
-                    }
-                    __nanosleep(sleep_ns);
-                    sleep_ns = sleep_ns < 2048 ? sleep_ns * 2 : sleep_ns;
-                }
-                atomicSub(db->idle, 1u);
-                if (slot != ~0ull) {
-                    // the writer reserved the slot with its words: it publishes shortly
-                    const unsigned long long t0 = gmk::now_ns();
-                    for (;;) {
-                        w = *(volatile unsigned long long*)(db->idx + slot);
+                const unsigned long long ticket = atomicAdd(db->claim, 1ull);
+                unsigned long long seen = ~0ull, t_seen = gmk::now_ns();
+                unsigned sleep_ns = 64;
+                for (uint32_t spin = 0;; ++spin) {
+                    if (ticket < db->idx_cap) {
+                        w = *(volatile unsigned long long*)(db->idx + ticket);
                         if (w) break;
-                        if (gmk::now_ns() - t0 > kPublishLimitNs) {
+                    }
+                    if ((spin & 7u) == 7u) {
+                        if (gmk::load_flag(o.stop)) { quit = 1; break; }
+                        const unsigned long long out = *(volatile unsigned long long*)db->outstanding;
+                        if (out + a.queue_len == 0) { quit = 1; break; }
+                        // safety net: the work left must change (a task ends or a
+                        // record is reserved) within the limit, else give up
+                        const unsigned long long sig = out + 0x9E3779B97F4A7C15ull *
+                                                       *(volatile unsigned long long*)db->tail;
+                        const unsigned long long now = gmk::now_ns();
+                        if (sig != seen) {
+                            seen = sig;
+                            t_seen = now;
+                        } else if (now - t_seen > kIdleLimitNs) {
                             atomicCAS(o.error, 0, gmk::TASK_E_TIMEOUT);
                             atomicExch(o.stop, 1);
                             quit = 1;
                             break;
                         }
-                        __nanosleep(64);
                     }
-                    __threadfence();
+                    __nanosleep(sleep_ns);
+                    sleep_ns = sleep_ns < 1024 ? sleep_ns * 2 : sleep_ns;
                 }
+                __threadfence();
             }
             quit = bcast(quit);
             if (quit) break;
             w = bcast(w);
-            const uint32_t* rec = db->words + (w - 1);
-            const GraphTask& G = use_graph<kBatch>(a, kBatch ? __ldcg(rec + 3) : 0u, t, o);
-            const unsigned long long nodes = run_record<kRec, kBits>(t, o, rec, sb, lim, db);
-            if (G.root_nodes && lane == 0)
-                atomicAdd(G.root_nodes + __ldcg(rec + gmk::warp::kRecHeader), nodes);
-            if (lane == 0) atomicAdd(db->outstanding, ~0ull);   // this record is finished
-            flush(t, o);
-            if (t.err) break;
-            continue;
+            rec = db->words + (w - 1);
+        } else {
+            if (lane == 0) atomicAdd(&a.rc->tasks_done, 1ull);
+            if (j < a.n_records) rec = a.cur_words + a.cur_idx[j];
         }
-        if (lane == 0) atomicAdd(&a.rc->tasks_done, 1ull);
-        if (j >= a.n_records) {
+        if (rec) {
+            // a record: of the previous round, or donated in this launch (one
+            // call site, so that run_record stays inlined)
+            const GraphTask& G = use_graph<kBatch>(a, kBatch ? __ldcg(rec + 3) : 0u, t, o);
+            // a round that winds down hands its queued records on unchanged
+            if (!(kRec && sb && draining(lim) && forward_record(t, *sb, rec))) {
+                const unsigned long long nodes = run_record<kRec, kBits>(t, o, rec, sb, lim, db);
+                if (G.root_nodes && lane == 0)
+                    atomicAdd(G.root_nodes + __ldcg(rec + gmk::warp::kRecHeader), nodes);
+            }
+        } else {
             const unsigned long long id = a.root_task_base + (j - a.n_records);
             uint32_t root, first, last, gi = 0;
             TaskEntry e{0, 0, 0, 0};
@@ -389,15 +380,6 @@ enumerate_warp_kernel(const __grid_constant__ WarpArgs a) {
             }
             const unsigned long long nodes = run_root<kRec, kBits>(t, o, root, first, last, sb, lim, db);
             if (G.root_nodes && lane == 0) atomicAdd(G.root_nodes + root, nodes);
-        } else {
-            const uint32_t* rec = a.cur_words + a.cur_idx[j];
-            const GraphTask& G = use_graph<kBatch>(a, kBatch ? rec[3] : 0u, t, o);
-            // a round that winds down hands its queued records on unchanged
-            if (!(kRec && sb && draining(lim) && forward_record(t, *sb, rec))) {
-                const unsigned long long nodes = run_record<kRec, kBits>(t, o, rec, sb, lim, db);
-                if (G.root_nodes && lane == 0)
-                    atomicAdd(G.root_nodes + rec[gmk::warp::kRecHeader], nodes);
-            }
         }
         if (db && lane == 0) atomicAdd(db->outstanding, ~0ull);   // this task is finished
         flush(t, o);
@@ -1016,7 +998,11 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
     std::vector<uint32_t> chunks(ng), cprs(ng);
     const uint32_t nsh = opts->nshards > 1 ? opts->nshards : 1u;
     const uint32_t sh = nsh > 1 ? opts->shard : 0u;
-    const bool planned = opts->schedule == GMK_SCHEDULE_ORDERED || nsh > 1 || opts->tasks;
+    // (a plain run given costs keeps one task per root and no splitting, but
+    // starts the largest predicted roots first: the static schedule with the
+    // learned order)
+    const bool planned = opts->schedule == GMK_SCHEDULE_ORDERED || nsh > 1 || opts->tasks ||
+                         (opts->schedule == GMK_SCHEDULE_PLAIN && jobs[0].task_cost);
     std::vector<gmk_task> plan;
     if (opts->tasks) {
         // the caller's list, as given (checked by gmk_enumerate)
@@ -1185,11 +1171,9 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
             a.share.idx_cap = dq_idx_cap;
             a.share.used = &rcd->dq_used;
             a.share.tail = &rcd->dq_tail;
-            a.share.head = &rcd->dq_head;
+            a.share.claim = &rcd->dq_claim;
             a.share.outstanding = &rcd->outstanding;
-            a.share.beat = &rcd->beat;
             a.share.donated = &rcd->donated;
-            a.share.idle = &rcd->idle;
             a.share.full = &rcd->dq_full;
             a.share.min_nodes = opts->donate_min_nodes ? opts->donate_min_nodes : kDefaultDonateMin;
         }
@@ -1806,7 +1790,8 @@ bool write_checkpoint(const char* path, const Checkpoint& c) {
 }
 
 uint64_t order_hash(const gmk_graph* g, const gmk_opts* o) {
-    if (o->schedule != GMK_SCHEDULE_ORDERED || !o->task_cost) return 0;
+    if ((o->schedule != GMK_SCHEDULE_ORDERED && o->schedule != GMK_SCHEDULE_PLAIN) || !o->task_cost)
+        return 0;
     uint64_t h = 0x51ED270B7A3C2D1Full;
     for (uint32_t i = 0; i < g->nl; ++i) {
         uint32_t bits;

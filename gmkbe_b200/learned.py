@@ -16,6 +16,7 @@ same with or without the model.
 from __future__ import annotations
 
 import ctypes
+import os
 
 import numpy as np
 
@@ -150,4 +151,89 @@ def predicted_costs(model: SubtreeModel, g: Graph, k: int) -> np.ndarray:
 
 
 __all__ = ["SubtreeModel", "root_features", "subtree_nodes", "target", "spearman",
-           "mean_relative_error", "makespan", "predicted_costs", "GmkError"]
+           "mean_relative_error", "makespan", "predicted_costs", "GmkError", "MODEL_PATH",
+           "training_set", "train_default", "load_default"]
+
+
+# ----------------------------------------------------------------------------- training
+MODEL_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "models", "subtree.npy")
+
+
+def _families():
+    """Training families: seeded graphs of the benchmark configurations'
+    generators, cut to induced prefixes whose complete enumeration finishes in
+    seconds (the full graphs have ~|E|.|V| maximal k-biplexes).  Each entry:
+    (name, builder(seed) -> graphgen.Graph, ks)."""
+    from . import graphgen as gg
+
+    def er200(seed):
+        return gg.erdos_renyi(200, 200, 0.05, seed)
+
+    def cl20k_sub(seed):
+        return gg.induced_prefix(gg.chung_lu(20_000, 50_000, 500_000, 2.1, seed, 2000), 5_000, 12_000)
+
+    def cl100k_sub(seed):
+        return gg.induced_prefix(gg.chung_lu(100_000, 300_000, 3_000_000, 2.2, seed), 8_000, 24_000)
+
+    def er60(seed):
+        return gg.erdos_renyi(30, 30, 0.3, seed)
+
+    return [("er200", er200, (1,)), ("cl20k_sub", cl20k_sub, (1, 2)),
+            ("cl100k_sub", cl100k_sub, (1, 2)), ("er60", er60, (2, 3))]
+
+
+def training_set(seeds=range(10, 20), watchdog_ms: int = 20_000, device: int = 0, log=None):
+    """(features, targets, info) over the training families: per root task, its
+    16 features and log1p of its search nodes, logged by complete runs."""
+    xs, ys, info = [], [], []
+    for name, build, ks in _families():
+        for seed in seeds:
+            h = build(seed)
+            if h.n_left in (0, h.n):
+                continue
+            with Graph.from_graph(h, device=device) as g:
+                for k in ks:
+                    try:
+                        nodes = subtree_nodes(g, k, watchdog_ms=watchdog_ms)
+                    except GmkError as e:
+                        if e.code != -8:      # watchdog: this case is skipped
+                            raise
+                        info.append({"family": name, "seed": seed, "k": k, "skipped": "watchdog"})
+                        continue
+                    xs.append(root_features(g, k))
+                    ys.append(target(nodes))
+                    info.append({"family": name, "seed": seed, "k": k, "roots": int(h.n_left),
+                                 "nodes": int(nodes.sum())})
+                    if log:
+                        log(info[-1])
+    return np.concatenate(xs), np.concatenate(ys), info
+
+
+def train_default(out_path: str = MODEL_PATH, epochs: int = 1500, lr: float = 3e-3, seed: int = 1,
+                  device: int = 0, log=None) -> dict:
+    """Trains the shipped model on the training families (seeds 10-19) with the
+    library's GPU kernels and saves its FP32 master weights."""
+    x, y, info = training_set(device=device, log=log)
+    m = SubtreeModel(device=device, seed=seed)
+    loss = m.train(x, y, epochs=epochs, lr=lr)
+    os.makedirs(os.path.dirname(out_path), exist_ok=True)
+    np.save(out_path, m.params())
+    return {"samples": int(len(y)), "loss": float(loss), "epochs": epochs, "lr": lr, "cases": info}
+
+
+def load_default(device: int = 0, path: str = MODEL_PATH) -> SubtreeModel:
+    """The shipped model (weights trained by train_default)."""
+    m = SubtreeModel(device=device, seed=0)
+    m.set_params(np.load(path))
+    return m
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="train the subtree-size model on the GPU")
+    ap.add_argument("--out", default=MODEL_PATH)
+    ap.add_argument("--epochs", type=int, default=1500)
+    a = ap.parse_args()
+    res = train_default(a.out, epochs=a.epochs, log=lambda r: print(json.dumps(r), flush=True))
+    print(json.dumps({k: v for k, v in res.items() if k != "cases"}), flush=True)

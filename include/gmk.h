@@ -70,7 +70,8 @@ void gmk_graph_free(gmk_graph* g);
 /* Schedules of the search tasks (one task = a root U vertex and a chunk of its
  * first-level children). */
 enum {
-    GMK_SCHEDULE_PLAIN = 0,    /* one task per root, roots in id order, no splitting */
+    GMK_SCHEDULE_PLAIN = 0,    /* one task per root, roots in id order (largest task_cost
+                                  first when one is given), no splitting */
     GMK_SCHEDULE_BATCHED = 1,  /* roots split into chunks, persistent work queue; unfinished
                                   search trees are split into the next round's tasks */
     GMK_SCHEDULE_ORDERED = 2   /* batched over planned tasks: roots split into chunks in
@@ -97,7 +98,8 @@ typedef struct {
                                  for the warp engine, 2048 for the thread engine */
     uint32_t watchdog_ms;     /* stop with GMK_E_TIMEOUT after this long; 0 = none */
     uint64_t out_words;       /* emit-mode record buffer (u32 words); 0 = automatic */
-    const float* task_cost;   /* GMK_SCHEDULE_ORDERED: one cost per root U vertex (n_left) */
+    const float* task_cost;   /* one cost per root U vertex (n_left): required by
+                                 GMK_SCHEDULE_ORDERED; orders the roots of a PLAIN run */
     uint32_t pair_limit;      /* node rules (shortcut, forcing, exclusion prune) run while
                                  (|S|+|C_U|)*(|S|+|C_V|) <= pair_limit; 0 = 4096 */
     uint32_t shard, nshards;  /* one GPU of several: run only this shard's tasks of the

@@ -1,20 +1,36 @@
 #!/usr/bin/env python
-"""Benchmark: maximal k-biplexes/s of the B200 enumerator on the Chung-Lu
-20k x 50k workload (gamma 2.1, max degree 2k, seed 2; k = 1, first 10^6
-results), one JSON line on rank 0.
+"""Benchmark: maximal k-biplexes/s of the B200 enumerator, learned+batched
+schedule against the plain GPU schedule, bit-exact result set; one JSON line
+on rank 0.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gmk|reference]
 
-A step is one enumeration of the workload up to the result limit.  `value` is
-device-timed (CUDA events around the kernel, graph already resident);
-`e2e` is the same metric through the public C ABI from pinned host CSR
-arrays, host->device copy and the statistics read-back inside the timed
-region.  L2 is flushed (256 MB write) between timed steps.  With N > 1 (one
-process per GPU under torchrun) every rank enumerates its own shard of the
-search tasks to the same result limit (weak scaling) and the slowest rank's
-time is used.  `--impl reference` times the reference's own CPU enumerator
-(BPPivot, built from its sources under oracle/_ref) on samples of the same
-workload; under torchrun only rank 0 runs it.
+Workload (the headline `value`): configuration 2's exactness case -- the
+Chung-Lu graph |U| = 20k, |V| = 50k (exponent 2.1, max degree 2k, seed 2),
+complete enumeration of the subgraph induced by its first 5k U and 12k V ids
+(tests/golden/cl20k_sub.graph.bin: 623 x 653 vertices, 660 edges, 245 860
+maximal 1-biplexes), k = 1.  A step is one complete enumeration; every step's
+set summary (count, sum and xor of per-result hashes) is checked against the
+golden summary of the reference's BPPivot output, so each timed step is
+bit-exact.  The schedule is learned+batched: the shipped subtree-size model
+(gmkbe_b200/models/subtree.npy) predicts every root's cost, the planner splits
+and orders the tasks by it, and the persistent kernel shares work inside the
+launch.  `value` is device-timed (CUDA events around the enumeration's
+launches, graph and predictions resident); `e2e` is the same metric through the
+public API from pinned host CSR arrays: upload, device CSR check, edge-hash
+build, root features, model prediction, planning, enumeration and read-back
+all inside the timed region.  L2 is flushed (256 MB write) between steps.
+
+Beside it: the plain schedule (one task per root, id order, no splitting) and
+the batched schedule without the model on the same graph; configuration 2's
+throughput run (full graph, first 10^6 results) and configurations 3 and 4
+(first 10^7 / 10^8 results) under the three schedules; and complete
+enumerations of configuration 1 and of subgraphs of configurations 3 and 4.
+`--impl reference` times the reference's own CPU enumerator (BPPivot, built
+from its sources under oracle/_ref) on the same complete enumeration.  With
+N > 1 (one process per GPU under torchrun) every rank runs its shard of the
+planned tasks (weak scaling in ranks, strong in work: the graph is the same)
+and the slowest rank's time is used.
 """
 from __future__ import annotations
 
@@ -33,11 +49,13 @@ sys.path.insert(0, ROOT)
 
 METRIC = "maximal k-biplexes/sec, learned+batched vs plain GPU, bit-exact result set"
 UNIT = "results/s"
-WORKLOAD = "cl20k"
-CONFIG_DESC = ("Chung-Lu bipartite |U|=20k |V|=50k ~500k edges (463,390 after dedup), "
-               "exponent 2.1 both sides, max degree 2k, seed 2; k=1, first 10^6 results")
-REF_STEP_SAMPLE = 100_000      # results per reference-arm step
-CPU_BASELINE_SAMPLE = 200_000  # results in the GPU arm's cpu_baseline leg
+WORKLOAD = "cl20k_sub"
+WORKLOAD_PATH = os.path.join(ROOT, "tests", "golden", "cl20k_sub.graph.bin")
+CONFIG_DESC = ("config 2: Chung-Lu bipartite |U|=20k |V|=50k ~500k edges, exponent 2.1, max "
+               "degree 2k, seed 2; complete enumeration of the subgraph induced by the first 5k U "
+               "and 12k V ids (623 x 653 vertices, 660 edges after dropping isolated vertices), "
+               "k=1, 245860 maximal 1-biplexes, bit-exact against BPPivot")
+K = 1
 
 
 def _peaks():
@@ -45,17 +63,34 @@ def _peaks():
     if os.path.exists(p):
         with open(p) as f:
             d = json.load(f)
-        return float(d["hbm_gbs"]), "measured"
-    return 6650.0, "fallback"
+        return float(d["hbm_gbs"]), "measured", float(d.get("sm_max_mhz", 1965.0))
+    return 6650.0, "fallback", 1965.0
 
 
-def _traffic_per_launch(kernel: str):
-    """DRAM bytes (read + write) per launch of `kernel` on this workload, from
-    the committed ncu summary (profiles/<kernel>_cl20k.json), or None."""
-    p = os.path.join(ROOT, "profiles", f"{kernel}_cl20k.json")
+def _profile(name: str):
+    """A committed ncu summary (profiles/<name>.json), or None."""
+    p = os.path.join(ROOT, "profiles", name + ".json")
     if os.path.exists(p):
         with open(p) as f:
-            return json.load(f).get("dram_bytes_per_launch")
+            return json.load(f)
+    return None
+
+
+def _algo_bytes(workload: str, k: int, limit: int):
+    """Algorithmic bytes of (workload, k, limit) counted by the host restatement
+    (profiles/algo_bytes.json, written by oracle/algo_bytes.py), or None."""
+    d = _profile("algo_bytes")
+    for c in (d or {}).get("cases", []):
+        if c["workload"] == workload and c["k"] == k and c["result_limit"] == limit:
+            return c
+    return None
+
+
+def _golden(name: str, k: int):
+    with open(os.path.join(ROOT, "tests", "golden", "golden.json")) as f:
+        for c in json.load(f)["cases"]:
+            if c["graph"] == name and c["k"] == k:
+                return c["count"], int(c["hash_sum"], 16), int(c["hash_xor"], 16)
     return None
 
 
@@ -127,25 +162,24 @@ def _dist():
 
 
 def run_reference(args, world, rank):
-    """Reference arm: BPPivot (the reference's CPU enumerator) on the same workload."""
+    """Reference arm: BPPivot (the reference's CPU enumerator) on the same
+    complete enumeration, one thread (it has no parallel mode)."""
     if rank != 0:
         return
     import oracle as O
-    from gmkbe_b200 import graphgen as gg
-    path = gg.cached_workload(WORKLOAD)
-    sample = min(args.limit, REF_STEP_SAMPLE)
-    config = {"workload": CONFIG_DESC, "k": args.k, "result_limit": args.limit,
-              "reference_sample_per_step": sample}
+    config = {"workload": CONFIG_DESC, "k": K, "result_limit": 0, "complete": True}
     if not os.path.exists(O.bppivot_path()):
         print(json.dumps({"impl": "reference", "unavailable":
                           "oracle/_ref/bppivot not built (reference sources absent at build time)"}))
         return
+    want = _golden(WORKLOAD, K)
     for _ in range(args.warmup):
-        O.run_bppivot(path, args.k, result_limit=1000)
+        O.run_bppivot(WORKLOAD_PATH, K)
     tot_res = tot_ms = 0
     walls = []
     for _ in range(args.steps):
-        r = O.run_bppivot(path, args.k, result_limit=sample)
+        r = O.run_bppivot(WORKLOAD_PATH, K)
+        assert r["count"] == want[0], (r["count"], want)
         tot_res += r["count"]
         tot_ms += max(r["branch_ms"], 1)
         walls.append(r["wall_s"])
@@ -155,24 +189,105 @@ def run_reference(args, world, rank):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic (seeded Chung-Lu, converter ordering)", "config": config,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
-                             "sample": f"first {sample} results of the workload per step, "
-                                       "BPPivot -q 1 -k 1 -n <sample>, branch time "
-                                       "(single-threaded; it has no parallel mode)"},
+                             "sample": "the complete enumeration per step (BPPivot -q 1 -k 1, "
+                                       "branch time; single-threaded, it has no parallel mode)"},
             "e2e": {"value": tot_res / sum(walls), "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def cpu_baseline(k):
+def cpu_baseline():
+    """BPPivot's complete enumeration of the workload on this host, one thread."""
     import oracle as O
-    from gmkbe_b200 import graphgen as gg
     if not os.path.exists(O.bppivot_path()):
         return None
-    r = O.run_bppivot(gg.cached_workload(WORKLOAD), k, result_limit=CPU_BASELINE_SAMPLE)
+    r = O.run_bppivot(WORKLOAD_PATH, K)
     return {"value": r["count"] / (max(r["branch_ms"], 1) / 1e3), "unit": UNIT, "cores": 1,
             "kind": "reference",
-            "sample": f"first {CPU_BASELINE_SAMPLE} results of the workload (BPPivot -q 1 -k {k} "
-                      f"-n {CPU_BASELINE_SAMPLE}), branch time {r['branch_ms']} ms, 1 thread"}
+            "sample": f"the complete enumeration ({r['count']} results), BPPivot -q 1 -k {K}, "
+                      f"branch time {r['branch_ms']} ms, wall {r['wall_s']:.2f} s, 1 thread",
+            "cpu": _cpu_model()}
+
+
+def _cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip() + f" ({os.cpu_count()} threads)"
+    except OSError:
+        pass
+    return None
+
+
+def _model(device: int):
+    """The shipped subtree-size model, or one trained now (and said so)."""
+    from gmkbe_b200 import learned as L
+    if os.path.exists(L.MODEL_PATH):
+        return L.load_default(device), "shipped (gmkbe_b200/models/subtree.npy)"
+    L.train_default(os.path.join(ROOT, "_graphs", "subtree.npy"), device=device)
+    return L.load_default(device, os.path.join(ROOT, "_graphs", "subtree.npy")), "trained at start"
+
+
+def _schedules(g, k, limit, cost, reps, flush, check=None, **kw):
+    """plain / batched / learned device times of one (graph, k, limit): the
+    median of `reps` runs after one untimed run each; sets compared."""
+    import torch
+    out, summ = {}, {}
+    for name, extra in (("learned", dict(schedule="ordered", task_cost=cost)),
+                        ("batched", dict(schedule="batched")), ("plain", dict(schedule="plain"))):
+        g.enumerate(k=k, result_limit=limit, **extra, **kw)
+        ms, st = [], None
+        for _ in range(reps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            st = g.enumerate(k=k, result_limit=limit, **extra, **kw)
+            ms.append(st.kernel_ms)
+        m = statistics.median(ms)
+        out[name] = {"ms": m, "results": st.count, "value": st.count / (m / 1e3),
+                     "rounds": st.rounds, "donations": st.donations, "tasks": st.tasks}
+        summ[name] = st.summary()
+    out["learned_vs_plain"] = out["plain"]["ms"] / out["learned"]["ms"]
+    out["batched_vs_plain"] = out["plain"]["ms"] / out["batched"]["ms"]
+    out["learned_vs_batched"] = out["batched"]["ms"] / out["learned"]["ms"]
+    if not limit:
+        out["same_set"] = len(set(summ.values())) == 1
+        if check is not None:
+            out["bit_exact_vs_golden"] = summ["learned"] == check
+    return out
+
+
+def _extras(model, flush, device):
+    """Configuration 2's throughput run and configurations 3-4, result-limited,
+    and complete enumerations of configuration 1 and of the config-3/4 family
+    subgraphs, under the three schedules."""
+    import gmkbe_b200 as G
+    from gmkbe_b200 import graphgen as gg
+    from gmkbe_b200 import learned as L
+    limited, complete = [], []
+    for name, k, limit in (("cl20k", 1, 1_000_000), ("cl100k", 2, 10_000_000),
+                           ("cl500k", 1, 100_000_000), ("cl500k", 2, 100_000_000)):
+        with G.Graph.load(gg.cached_workload(name), device=device) as g:
+            r = _schedules(g, k, limit, L.predicted_costs(model, g, k), 3, flush)
+            r.update(workload=name, k=k, result_limit=limit)
+            limited.append(r)
+    for name, k, sub in COMPLETE_CASES:
+        h = gg.read_graph_bin(os.path.join(ROOT, "tests", "golden", name + ".graph.bin")) \
+            if sub is None else gg.induced_prefix(gg.read_graph_bin(gg.cached_workload(name)), *sub)
+        with G.Graph.from_graph(h, device=device) as g:
+            r = _schedules(g, k, 0, L.predicted_costs(model, g, k), 3, flush,
+                           check=_golden(name, k) if sub is None else None)
+            r.update(workload=name if sub is None else f"{name} induced {sub[0]}x{sub[1]}", k=k,
+                     vertices=[h.n_left, h.n - h.n_left], edges=h.n_edges)
+            complete.append(r)
+    return limited, complete
+
+
+# complete enumerations beside the headline: (workload, k, induced prefix or None).  As for
+# configuration 2's exactness case, a prefix is the subgraph induced by the first U and V ids
+# (the converter's order: lowest degrees first), sized so that the run ends in well under a second.
+COMPLETE_CASES = [("er200", 1, None), ("cl100k", 1, (20000, 60000)), ("cl100k", 2, (4000, 12000)),
+                  ("cl500k", 2, (20000, 40000)), ("cl500k", 3, (10000, 20000))]
 
 
 def run_gmk(args, world, rank, local):
@@ -180,76 +295,73 @@ def run_gmk(args, world, rank, local):
     import torch
     import gmkbe_b200 as G
     from gmkbe_b200 import graphgen as gg
+    from gmkbe_b200 import learned as L
 
     torch.cuda.set_device(local)
     if world > 1:
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    path = gg.cached_workload(WORKLOAD) if rank == 0 else None
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
-        path = gg.cached_workload(WORKLOAD)
-    host = gg.read_graph_bin(path)
+    host = gg.read_graph_bin(WORKLOAD_PATH)
     off = torch.from_numpy(host.offsets.astype(np.uint32).view(np.int32)).pin_memory()
     adj = torch.from_numpy(host.adj.view(np.int32)).pin_memory()
     off_np = off.numpy().view(np.uint32)
     adj_np = adj.numpy().view(np.uint32)
-    h2d = 4 * (off_np.size + adj_np.size)
-    kw = dict(k=args.k, result_limit=args.limit, schedule=args.schedule, engine=args.engine)
-    if world > 1:
-        kw.update(shard=rank, nshards=world)
+    shard = dict(shard=rank, nshards=world) if world > 1 else {}
 
     def barrier():
         if world > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
-    dg = G.Graph.from_csr(off_np, adj_np, host.n, host.n_left, device=local)
+    model, model_src = _model(local)
     flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    want = _golden(WORKLOAD, K)
+    dg = G.Graph.from_csr(off_np, adj_np, host.n, host.n_left, device=local)
+    cost = L.predicted_costs(model, dg, K)        # the learned schedule's input, resident
+    kw = dict(k=K, schedule="ordered", task_cost=cost, **shard)
     for _ in range(args.warmup):
         dg.enumerate(**kw)
     barrier()
     clocks = ClockSampler(local)
     clocks.start()
     t_clk0 = time.perf_counter()
-    ms, count, algo, launches = [], 0, 0, 0
+    ms, count, launches, exact = [], 0, 0, True
     for _ in range(args.steps):
-        flush_buf.zero_()          # L2 flush, outside the timed kernel
+        flush_buf.zero_()          # L2 flush, outside the timed kernels
         torch.cuda.synchronize()
         st = dg.enumerate(**kw)
         ms.append(st.kernel_ms)
         count += st.count
-        algo += st.algo_bytes
         launches += st.rounds
+        if world == 1:
+            exact &= st.summary() == want
     barrier()
     clk = clocks.stop(t_clk0, time.perf_counter())
-    # the plain static schedule on the same GPU (one task per root, no splitting)
-    plain = None
-    if args.schedule != "plain" and not args.no_plain:
-        flush_buf.zero_()
-        torch.cuda.synchronize()
-        sp = dg.enumerate(**dict(kw, schedule="plain"))
-        plain = {"value": sp.count / (sp.kernel_ms / 1e3), "ms": sp.kernel_ms,
-                 "results": sp.count}
-    # end to end through the C ABI: host CSR -> device, enumerate, read back.
-    # W untimed steps first, like the device arm (the first upload of a second
-    # graph fills the device buffer cache)
+    if world > 1:
+        from gmkbe_b200.shard import combine_summary
+        exact = combine_summary(*st.summary(), device=f"cuda:{local}") == want
+    # the same graph under the plain and the batched schedule (this rank's shard)
+    sched = _schedules(dg, K, 0, cost, min(args.steps, 5), flush_buf, check=want, **shard)
+    # end to end through the public API, from pinned host arrays: upload + CSR
+    # check + edge hash, root features + model prediction, planning,
+    # enumeration, statistics read-back
     for _ in range(args.warmup):
         with G.Graph.from_csr(off_np, adj_np, host.n, host.n_left, device=local) as g2:
-            g2.enumerate(**kw)
+            g2.enumerate(k=K, schedule="ordered", task_cost=L.predicted_costs(model, g2, K), **shard)
     barrier()
-    e2e_s, e2e_rounds = 0.0, 0
+    e2e_s, e2e_rounds, e2e_tasks = 0.0, 0, 0
     for _ in range(args.steps):
         flush_buf.zero_()
         barrier()
         t0 = time.perf_counter()
         g2 = G.Graph.from_csr(off_np, adj_np, host.n, host.n_left, device=local)
-        st2 = g2.enumerate(**kw)
+        c2 = L.predicted_costs(model, g2, K)
+        st2 = g2.enumerate(k=K, schedule="ordered", task_cost=c2, **shard)
         g2.close()
         e2e_s += time.perf_counter() - t0
         e2e_rounds += st2.rounds
+        e2e_tasks += st2.tasks
     barrier()
     tot_ms = sum(ms)
     if world > 1:
@@ -260,38 +372,56 @@ def run_gmk(args, world, rank, local):
         count_all = float(combine_summary(count, 0, 0, device=dev)[0])
     else:
         tot_ms_max, e2e_max, count_all = tot_ms, e2e_s, float(count)
-    # counters read back after every round: 32 B round counters + 88 B totals
-    d2h = 120 * e2e_rounds / max(1, args.steps)
+    # bytes copied per end-to-end step: host -> device the CSR (n+1 offsets and
+    # 2|E| ids), the features for the model (n_left x 16 FP32) and the task
+    # table (16 B a task); device -> host the root features (n_left x 16 FP16),
+    # the predictions (n_left FP32), the CSR check (16 B) and per launch the
+    # round counters (512 B) and totals (88 B)
+    nl = host.n_left
+    h2d = 4 * (off_np.size + adj_np.size) + 64 * nl + 16 * e2e_tasks / args.steps
+    d2h = 32 * nl + 4 * nl + 16 + 600 * e2e_rounds / args.steps
     if rank == 0:
-        peak, peak_kind = _peaks()
-        achieved = (algo / args.steps) / (tot_ms / args.steps / 1e3) / 1e9
+        peak, peak_kind, sm_max = _peaks()
+        ab = _algo_bytes(WORKLOAD, K, 0)
+        prof = _profile("enumerate_warp_kernel_cl20k_sub") or {}
+        mean_ms = tot_ms / args.steps
+        achieved = (ab["algo_bytes"] / world / (mean_ms / 1e3) / 1e9) if ab else None
         line = {
             "metric": METRIC, "value": count_all / (tot_ms_max / 1e3), "unit": UNIT,
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": tot_ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded Chung-Lu, converter ordering)",
-            "config": {"workload": CONFIG_DESC, "k": args.k, "result_limit": args.limit,
-                       "schedule": args.schedule, "l2": "flushed between steps (256 MB write)",
+            "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded Chung-Lu, converter ordering)",
+            "config": {"workload": CONFIG_DESC, "k": K, "result_limit": 0, "complete": True,
+                       "schedule": "learned+batched (ordered planner over the model's predicted "
+                                   "subtree sizes, in-launch work sharing)",
+                       "model": model_src, "l2": "flushed between steps (256 MB write)",
                        "parallelism": f"task shards x{world}" if world > 1 else "1 GPU"},
+            "bit_exact": bool(exact),
             "e2e": {"value": count_all / e2e_max, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak,
-                         "traffic": _traffic_per_launch("enumerate_warp_kernel" if args.engine == "warp"
-                                                        else "enumerate_kernel"),
-                         "peak_source": peak_kind,
-                         "kernel": ("enumerate_warp_kernel" if args.engine == "warp"
-                                    else "enumerate_kernel"),
-                         "algorithmic_bytes_per_launch": algo / args.steps},
+            "learned_vs_plain": sched["learned_vs_plain"],
+            "schedules": sched,
+            "roofline": {
+                "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak if achieved else None,
+                "traffic": prof.get("dram_bytes_per_launch"), "peak_source": peak_kind,
+                "kernel": "enumerate_warp_kernel",
+                "algorithmic_bytes_per_step": ab["algo_bytes"] if ab else None,
+                "algorithmic_bytes_source": "profiles/algo_bytes.json (oracle/algo_bytes.py)",
+                "l2_hit_rate": prof.get("l2_hit_rate_pct"),
+                "issue_active_frac": prof.get("issue_active_frac"),
+                "warp_inst_per_launch": prof.get("warp_inst_per_launch"),
+                "binding_ceiling": prof.get("binding_ceiling")},
             "clocks": clk,
-            "stats": {"nodes_per_step": st.nodes, "tasks": st.tasks, "tasks_done": st.tasks_done,
-                      "threads": st.threads, "rounds_per_step": launches / args.steps,
-                      "engine": args.engine},
-            "plain_schedule": plain,
+            "stats": {"nodes_per_step": st.nodes, "tasks": st.tasks, "threads": st.threads,
+                      "rounds_per_step": launches / args.steps, "donations": st.donations},
         }
+        if world == 1 and not args.no_extras:
+            line["limited"], line["complete_runs"] = _extras(model, flush_buf, local)
         if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(args.k)
+            line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line), flush=True)
     dg.close()
     if world > 1:
@@ -304,12 +434,9 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gmk", choices=["gmk", "reference"])
-    ap.add_argument("--k", type=int, default=1)
-    ap.add_argument("--limit", type=int, default=1_000_000)
-    ap.add_argument("--schedule", default="batched", choices=["plain", "batched"])
-    ap.add_argument("--engine", default="warp", choices=["warp", "thread"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-plain", action="store_true", help="skip the plain-schedule comparison")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the result-limited configurations and the complete-run table")
     args = ap.parse_args()
     world, rank, local = _dist()
     if args.impl == "reference":

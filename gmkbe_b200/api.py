@@ -123,11 +123,12 @@ def load_library(path: str = LIB_PATH):
     lib.gmk_result_hash.argtypes = [P32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                                     ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
     lib.gmk_result_hash.restype = None
-    lib.gmk_root_costs.argtypes = [ctypes.c_void_p, PF]
-    lib.gmk_plan_tasks.argtypes = [ctypes.c_uint32, ctypes.c_uint32, PF, ctypes.c_uint32,
-                                   ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint32,
-                                   ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(_Task),
-                                   ctypes.POINTER(ctypes.c_uint64)]
+    if hasattr(lib, "gmk_plan_tasks"):   # (a library build from before the planner lacks them)
+        lib.gmk_root_costs.argtypes = [ctypes.c_void_p, PF]
+        lib.gmk_plan_tasks.argtypes = [ctypes.c_uint32, ctypes.c_uint32, PF, ctypes.c_uint32,
+                                       ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint32,
+                                       ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(_Task),
+                                       ctypes.POINTER(ctypes.c_uint64)]
     lib.gmk_strerror.restype = ctypes.c_char_p
     lib.gmk_last_cuda_error.restype = ctypes.c_char_p
     _lib = lib

@@ -11,26 +11,63 @@
 // --engine warp|thread, --checkpoint FILE [--batch-roots N] (resumable run:
 // the file is rewritten after every batch of roots and a restarted command
 // continues from it).
+#include <charconv>
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "gmk.h"
 
 namespace {
 
+// Result lines in the reference's format (include/output.cuh:102-145):
+// "Result <n>: X: x1 x2 | Y: y1 y2 \n" -- X ids joined by single spaces, each Y
+// id followed by one.  Lines are formatted into a 4 MiB buffer and written
+// with fwrite when it fills (one printf per id measured 4-5x slower).
 struct Printer {
     unsigned long long n = 0;
+    std::vector<char> buf = std::vector<char>(4u << 20);
+    size_t len = 0;
+    FILE* out = stdout;
+
+    void flush() {
+        if (len) std::fwrite(buf.data(), 1, len, out);
+        len = 0;
+    }
+    char* room(size_t need) {
+        if (len + need > buf.size()) flush();
+        if (need > buf.size()) buf.resize(need);
+        return buf.data() + len;
+    }
+    static char* put_u64(char* p, unsigned long long v) {
+        return std::to_chars(p, p + 24, v).ptr;
+    }
 };
 
 int print_result(void* user, const uint32_t* x, uint32_t nx, const uint32_t* y, uint32_t ny) {
-    Printer* p = static_cast<Printer*>(user);
-    std::printf("Result %llu: X:", ++p->n);
-    for (uint32_t i = 0; i < nx; ++i) std::printf(" %u", x[i]);
-    std::printf(" | Y: ");
-    for (uint32_t i = 0; i < ny; ++i) std::printf("%u ", y[i]);
-    std::printf("\n");
+    Printer* pr = static_cast<Printer*>(user);
+    // at most 11 bytes per id, 40 for the fixed text and the counter
+    char* p = pr->room(64 + 11ull * (nx + ny));
+    char* const start = p;
+    std::memcpy(p, "Result ", 7);
+    p = Printer::put_u64(p + 7, ++pr->n);
+    std::memcpy(p, ": X:", 4);
+    p += 4;
+    for (uint32_t i = 0; i < nx; ++i) {
+        *p++ = ' ';
+        p = Printer::put_u64(p, x[i]);
+    }
+    std::memcpy(p, " | Y: ", 6);
+    p += 6;
+    for (uint32_t i = 0; i < ny; ++i) {
+        p = Printer::put_u64(p, y[i]);
+        *p++ = ' ';
+    }
+    *p++ = '\n';
+    pr->len += (size_t)(p - start);
     return 0;
 }
 
@@ -76,6 +113,7 @@ int main(int argc, char** argv) {
         else if (!std::strcmp(argv[i], "--schedule")) {
             const char* s = val("--schedule");
             o.schedule = !std::strcmp(s, "plain") ? GMK_SCHEDULE_PLAIN : GMK_SCHEDULE_BATCHED;
+            if (std::strcmp(s, "plain") && std::strcmp(s, "batched")) { usage(); return 2; }
         } else if (!std::strcmp(argv[i], "-h") || !std::strcmp(argv[i], "--help")) {
             usage();
             return 0;
@@ -94,27 +132,39 @@ int main(int argc, char** argv) {
     uint32_t n = 0, nl = 0;
     uint64_t m = 0;
     gmk_graph_info(g, &n, &nl, &m);
-    std::printf("Graph size: %u, edge num: %llu, bipartite index: %u, k = %u\n", n,
+    // the reference's header line (src/main.cu:1593-1595; its theta is fixed to 1)
+    std::printf("Graph size: %u, edge num: %llu, bipartite index: %u, k = %u, theta = 1\n", n,
                 (unsigned long long)m, nl, o.k);
+    std::fflush(stdout);
     Printer p;
     o.emit = quiet ? 1 : 0;
     gmk_stats st;
+    const auto t0 = std::chrono::steady_clock::now();
     // results stream through the library's record buffers; no retry is needed
     rc = checkpoint.empty() ? gmk_enumerate(g, &o, quiet ? print_result : nullptr, &p, &st)
                             : gmk_enumerate_resumable(g, &o, checkpoint.c_str(), batch_roots, 0,
                                                       quiet ? print_result : nullptr, &p, &st);
+    p.flush();
+    std::fflush(stdout);
+    const double wall_ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     if (rc) {
         std::fprintf(stderr, "gmk: %s (%s)\n", gmk_strerror(rc), gmk_last_cuda_error());
         gmk_graph_free(g);
         return 1;
     }
-    std::printf("Running Time: %.3f ms\n", st.kernel_ms);
+    // the double in its shortest round-trip form, as the reference's fmt prints it
+    // (src/main.cu:1709)
+    char ms[64];
+    *std::to_chars(ms, ms + sizeof(ms) - 1, st.kernel_ms).ptr = 0;
+    std::printf("Running Time: %s ms\n", ms);
     if (stats)
         std::printf("results %llu hash_sum %016llx hash_xor %016llx nodes %llu tasks %llu threads %u "
-                    "rounds %u\n",
+                    "rounds %u lines %llu wall_ms %.3f lines_per_s %.0f\n",
                     (unsigned long long)st.count, (unsigned long long)st.hash_sum,
                     (unsigned long long)st.hash_xor, (unsigned long long)st.nodes,
-                    (unsigned long long)st.tasks, st.threads, st.rounds);
+                    (unsigned long long)st.tasks, st.threads, st.rounds, p.n, wall_ms,
+                    wall_ms > 0 ? p.n / (wall_ms / 1e3) : 0.0);
     gmk_graph_free(g);
     return 0;
 }

@@ -163,50 +163,61 @@ def _families():
     """Training families: seeded graphs of the benchmark configurations'
     generators, cut to induced prefixes whose complete enumeration finishes in
     seconds (the full graphs have ~|E|.|V| maximal k-biplexes).  Each entry:
-    (name, builder(seed) -> graphgen.Graph, ks)."""
+    (name, builder(seed) -> graphgen.Graphs, the ks of each graph, seeds)."""
     from . import graphgen as gg
 
     def er200(seed):
-        return gg.erdos_renyi(200, 200, 0.05, seed)
+        return [gg.erdos_renyi(200, 200, 0.05, seed)]
 
-    def cl20k_sub(seed):
-        return gg.induced_prefix(gg.chung_lu(20_000, 50_000, 500_000, 2.1, seed, 2000), 5_000, 12_000)
+    def cl20k(seed):
+        return [gg.induced_prefix(gg.chung_lu(20_000, 50_000, 500_000, 2.1, seed, 2000),
+                                  5_000, 12_000)]
 
-    def cl100k_sub(seed):
-        return gg.induced_prefix(gg.chung_lu(100_000, 300_000, 3_000_000, 2.2, seed), 8_000, 24_000)
+    def cl100k(seed):
+        full = gg.chung_lu(100_000, 300_000, 3_000_000, 2.2, seed)
+        return [gg.induced_prefix(full, 20_000, 60_000), gg.induced_prefix(full, 4_000, 12_000)]
 
-    def er60(seed):
-        return gg.erdos_renyi(30, 30, 0.3, seed)
+    def cl500k(seed):
+        full = gg.chung_lu(500_000, 1_000_000, 20_000_000, 2.0, seed)
+        return [gg.induced_prefix(full, 20_000, 40_000), gg.induced_prefix(full, 10_000, 20_000)]
 
-    return [("er200", er200, (1,)), ("cl20k_sub", cl20k_sub, (1, 2)),
-            ("cl100k_sub", cl100k_sub, (1, 2)), ("er60", er60, (2, 3))]
+    # (name, builder, k of each graph the builder returns, seeds)
+    return [("er200", er200, ((1,),), range(10, 20)),
+            ("cl20k", cl20k, ((1,),), range(10, 20)),
+            ("cl100k", cl100k, ((1,), (2,)), range(10, 20)),
+            ("cl500k", cl500k, ((2,), (3,)), range(10, 13))]
 
 
-def training_set(seeds=range(10, 20), watchdog_ms: int = 20_000, device: int = 0, log=None):
+def training_set(watchdog_ms: int = 20_000, device: int = 0, log=None):
     """(features, targets, info) over the training families: per root task, its
     16 features and log1p of its search nodes, logged by complete runs."""
     xs, ys, info = [], [], []
-    for name, build, ks in _families():
+    for name, build, kss, seeds in _families():
         for seed in seeds:
-            h = build(seed)
-            if h.n_left in (0, h.n):
-                continue
-            with Graph.from_graph(h, device=device) as g:
-                for k in ks:
-                    try:
-                        nodes = subtree_nodes(g, k, watchdog_ms=watchdog_ms)
-                    except GmkError as e:
-                        if e.code != -8:      # watchdog: this case is skipped
-                            raise
-                        info.append({"family": name, "seed": seed, "k": k, "skipped": "watchdog"})
-                        continue
-                    xs.append(root_features(g, k))
-                    ys.append(target(nodes))
-                    info.append({"family": name, "seed": seed, "k": k, "roots": int(h.n_left),
-                                 "nodes": int(nodes.sum())})
-                    if log:
-                        log(info[-1])
+            for h, ks in zip(build(seed), kss):
+                if h.n_left in (0, h.n):
+                    continue
+                _log_graph(h, ks, name, seed, watchdog_ms, device, xs, ys, info, log)
     return np.concatenate(xs), np.concatenate(ys), info
+
+
+def _log_graph(h, ks, name, seed, watchdog_ms, device, xs, ys, info, log):
+    """Appends graph h's features and logged subtree sizes for each k."""
+    with Graph.from_graph(h, device=device) as g:
+        for k in ks:
+            try:
+                nodes = subtree_nodes(g, k, watchdog_ms=watchdog_ms)
+            except GmkError as e:
+                if e.code != -8:      # watchdog: this case is skipped
+                    raise
+                info.append({"family": name, "seed": seed, "k": k, "skipped": "watchdog"})
+                continue
+            xs.append(root_features(g, k))
+            ys.append(target(nodes))
+            info.append({"family": name, "seed": seed, "k": k, "roots": int(h.n_left),
+                         "nodes": int(nodes.sum())})
+            if log:
+                log(info[-1])
 
 
 def train_default(out_path: str = MODEL_PATH, epochs: int = 1500, lr: float = 3e-3, seed: int = 1,

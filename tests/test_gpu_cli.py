@@ -1,0 +1,89 @@
+"""The drop-in executable `gmk` (same -f/-k/-r/-q/-d flags as the reference's
+gmkbpe, src/main.cu:1719-1775) on the GPU: its `-q 1` result lines have the
+reference's format (include/output.cuh:102-145: "Result <n>: X: x1 x2 | Y:
+y1 y2 "), are numbered 1..N, and hold exactly BPPivot's result set; the header
+and `Running Time:` lines follow src/main.cu:1593 and :1709; -r stops at the
+limit; and the buffered writer's rate is reported."""
+import os
+import re
+import subprocess
+
+import pytest
+
+from conftest import GOLDEN, ROOT, golden_graph_path
+
+pytestmark = pytest.mark.gpu
+
+CLI = os.path.join(ROOT, "gmkbe_b200", "gmk")
+RESULT = re.compile(r"^Result (\d+): X:((?: \d+)+) \| Y: ((?:\d+ )+)$")
+HEADER = re.compile(r"^Graph size: (\d+), edge num: (\d+), bipartite index: (\d+), k = (\d+), "
+                    r"theta = 1$")
+RUNNING = re.compile(r"^Running Time: (\d+(?:\.\d+)?(?:e[-+]?\d+)?) ms$")
+
+
+def _run(*args):
+    p = subprocess.run([CLI, *args], capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr
+    return p.stdout.splitlines()
+
+
+def _parse(lines):
+    results, other = [], []
+    for line in lines:
+        m = RESULT.match(line)
+        if m:
+            results.append((int(m.group(1)), tuple(int(v) for v in m.group(2).split()),
+                            tuple(int(v) for v in m.group(3).split())))
+        else:
+            other.append(line)
+    return results, other
+
+
+def test_result_lines_match_the_reference_format_and_set():
+    lines = _run("-f", golden_graph_path("southernwomen"), "-k", "1", "-q", "1", "--all")
+    results, other = _parse(lines)
+    assert HEADER.match(other[0]), other[0]
+    assert RUNNING.match(other[-1]), other[-1]
+    assert len(other) == 2, other
+    assert [n for n, _, _ in results] == list(range(1, len(results) + 1))
+    got = {(x, y) for _, x, y in results}
+    want = set()
+    with open(os.path.join(GOLDEN, "southernwomen_k1_sets.txt")) as f:
+        for line in f:
+            xs, ys = line.split("|")
+            want.add((tuple(int(v) for v in xs.split()), tuple(int(v) for v in ys.split())))
+    assert len(results) == len(got) == 1256
+    assert got == want
+    # ids ascending within each side, X in U and Y in V
+    n, _, nl, _ = (int(v) for v in HEADER.match(other[0]).groups())
+    for _, x, y in results:
+        assert list(x) == sorted(x) and list(y) == sorted(y)
+        assert x[-1] < nl <= y[0] and y[-1] < n
+
+
+def test_result_limit_and_quiet_mode():
+    results, other = _parse(_run("-f", golden_graph_path("southernwomen"), "-k", "2", "-q", "1",
+                                 "-r", "100"))
+    assert len(results) == 100 and len({(x, y) for _, x, y in results}) == 100
+    results, other = _parse(_run("-f", golden_graph_path("southernwomen"), "-k", "2", "-r", "100"))
+    assert results == [] and RUNNING.match(other[-1])
+
+
+def test_million_line_output_rate(golden, tmp_path):
+    # er200, k = 1: 1 891 002 lines; the set summary of the printed run equals
+    # the golden one and the writer's lines per second are reported
+    case = next(c for c in golden["cases"] if c["graph"] == "er200" and c["k"] == 1)
+    out = tmp_path / "out.txt"
+    with open(out, "w") as f:
+        p = subprocess.run([CLI, "-f", golden_graph_path("er200"), "-k", "1", "-q", "1", "--all",
+                            "--stats"], stdout=f, stderr=subprocess.PIPE, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr
+    tail = subprocess.run(["tail", "-n", "2", str(out)], capture_output=True, text=True).stdout
+    stats = dict(zip(*[iter(tail.splitlines()[-1].split())] * 2))
+    assert int(stats["results"]) == int(stats["lines"]) == case["count"]
+    assert int(stats["hash_sum"], 16) == int(case["hash_sum"], 16)
+    assert int(stats["hash_xor"], 16) == int(case["hash_xor"], 16)
+    wc = subprocess.run(["wc", "-l", str(out)], capture_output=True, text=True).stdout.split()[0]
+    assert int(wc) == case["count"] + 3
+    print(f"gmk -q 1: {stats['lines']} lines, {float(stats['lines_per_s']) / 1e6:.2f} M lines/s "
+          f"(wall {stats['wall_ms']} ms)")

@@ -28,7 +28,7 @@ EXPORTS = ("gmk_graph_load", "gmk_graph_from_csr", "gmk_graph_info", "gmk_graph_
            "gmk_enumerate_noalloc", "gmk_result_hash", "gmk_strerror", "gmk_last_cuda_error",
            "gmk_abi_version", "gmk_root_features", "gmk_mlp_create", "gmk_mlp_free",
            "gmk_mlp_params", "gmk_mlp_gradient", "gmk_mlp_train", "gmk_mlp_predict",
-           "gmk_root_costs", "gmk_plan_tasks")
+           "gmk_root_costs", "gmk_plan_tasks", "gmk_graph_set_hash_load")
 
 SCHEDULES = {"plain": 0, "batched": 1, "ordered": 2}
 ENGINES = {"warp": 0, "thread": 1}
@@ -57,7 +57,8 @@ class _Opts(ctypes.Structure):
                 ("root_begin", ctypes.c_uint32), ("root_end", ctypes.c_uint32),
                 ("root_nodes", ctypes.POINTER(ctypes.c_uint64)),
                 ("donate_min_nodes", ctypes.c_uint32), ("no_sharing", ctypes.c_int32),
-                ("tasks", ctypes.c_void_p), ("n_tasks", ctypes.c_uint64)]
+                ("tasks", ctypes.c_void_p), ("n_tasks", ctypes.c_uint64),
+                ("tasks_per_worker", ctypes.c_uint32), ("bits_min_list", ctypes.c_uint32)]
 
 
 class _Stats(ctypes.Structure):
@@ -101,6 +102,7 @@ def load_library(path: str = LIB_PATH):
     lib.gmk_enumerate.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Opts), SINK, ctypes.c_void_p,
                                   ctypes.POINTER(_Stats)]
     lib.gmk_enumerate_batch.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_uint32, P32,
+                                        ctypes.POINTER(ctypes.c_uint64),
                                         ctypes.POINTER(ctypes.POINTER(ctypes.c_float)),
                                         ctypes.POINTER(_Opts), ctypes.POINTER(_Stats)]
     lib.gmk_enumerate_resumable.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Opts), ctypes.c_char_p,
@@ -123,6 +125,8 @@ def load_library(path: str = LIB_PATH):
     lib.gmk_result_hash.argtypes = [P32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                                     ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
     lib.gmk_result_hash.restype = None
+    if hasattr(lib, "gmk_graph_set_hash_load"):
+        lib.gmk_graph_set_hash_load.argtypes = [ctypes.c_void_p, ctypes.c_uint32]
     if hasattr(lib, "gmk_plan_tasks"):   # (a library build from before the planner lacks them)
         lib.gmk_root_costs.argtypes = [ctypes.c_void_p, PF]
         lib.gmk_plan_tasks.argtypes = [ctypes.c_uint32, ctypes.c_uint32, PF, ctypes.c_uint32,
@@ -161,10 +165,11 @@ class Stats:
         return self.count, self.hash_sum, self.hash_xor
 
 
-def enumerate_batch(graphs, ks, schedule: str = "batched", task_costs=None, **tuning) -> list:
-    """gmk_enumerate_batch: full enumeration of several graphs (all on one
-    device) in one run of launches; ks[i] is graph i's k.  Returns one Stats
-    per graph."""
+def enumerate_batch(graphs, ks, schedule: str = "batched", task_costs=None, limits=None,
+                    **tuning) -> list:
+    """gmk_enumerate_batch: several graphs (all on one device) in one run of
+    launches; ks[i] is graph i's k, limits[i] its result cap (None: complete
+    enumeration of every graph).  Returns one Stats per graph."""
     lib = load_library()
     n = len(graphs)
     o, _ = graphs[0]._opts(int(ks[0]), 0, schedule, tuning.get("chunk", 0), tuning.get("threads", 0),
@@ -183,8 +188,12 @@ def enumerate_batch(graphs, ks, schedule: str = "batched", task_costs=None, **tu
             costs_keep.append(c)
             costs[i] = c.ctypes.data_as(PF)
     outs = (_Stats * n)()
+    lim = None
+    if limits is not None:
+        larr = np.ascontiguousarray(limits, dtype=np.uint64)
+        lim = larr.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
     _check(lib.gmk_enumerate_batch(hs, n, karr.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
-                                   costs, ctypes.byref(o), outs))
+                                   lim, costs, ctypes.byref(o), outs))
     return [Graph._stats(outs[i], None) for i in range(n)]
 
 
@@ -231,6 +240,10 @@ class Graph:
         n, nl, m = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint64()
         _check(lib.gmk_graph_info(self._h, ctypes.byref(n), ctypes.byref(nl), ctypes.byref(m)))
         self.n, self.n_left, self.adj_len = n.value, nl.value, m.value
+
+    def set_hash_load(self, load_pct: int) -> None:
+        """gmk_graph_set_hash_load: rebuild the edge hash at this maximum load (%)."""
+        _check(load_library().gmk_graph_set_hash_load(self._h, load_pct))
 
     def root_costs(self) -> np.ndarray:
         """gmk_root_costs: the 2-hop cost proxy of every root (float32, n_left)."""
@@ -332,7 +345,8 @@ class Graph:
                   task_cost=None, sink=None, shard: int = 0, nshards: int = 1,
                   engine: str = "warp", split_min_nodes: int = 0, root_begin: int = 0,
                   root_end: int = 0, root_nodes=None, out_words: int = 0,
-                  donate_min_nodes: int = 0, sharing: bool = True, tasks=None) -> Stats:
+                  donate_min_nodes: int = 0, sharing: bool = True, tasks=None,
+                  tasks_per_worker: int = 0, bits_min_list: int = 0) -> Stats:
         """Enumerate maximal k-biplexes.  collect=True returns the result list
         (sorted X, Y tuples) in Stats.results; `sink(x, y)` is called per
         result otherwise (return True to stop).  root_nodes: a uint64 numpy
@@ -348,6 +362,7 @@ class Graph:
             o.root_nodes = root_nodes.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
         o.donate_min_nodes = donate_min_nodes
         o.no_sharing = 0 if sharing else 1
+        o.tasks_per_worker, o.bits_min_list = tasks_per_worker, bits_min_list
         task_buf = None
         if tasks is not None:
             # an explicit task list (structured array from plan_tasks, or rows of

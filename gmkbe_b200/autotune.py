@@ -1,14 +1,24 @@
-"""Autotuner for the warp engine's schedule knobs.
+"""Autotuner for the warp engine: the knobs north_star names, per graph.
 
-For one (graph, k) it times short result-limited enumerations over a small
-grid of settings and keeps the fastest:
-  * chunk           first-level children per root task (0 = about 8 tasks per warp);
-  * split_min_nodes nodes a task must have run before a hungry round splits it;
-  * pair_limit      largest |S u C_U| x |S u C_V| at which the node rules
-                    (shortcut, forcing, exclusion prune) run.
-None of them changes the result set, only the schedule and the pruning
-effort.  Winners are cached in a JSON file keyed by the graph's fingerprint,
-k and the result limit, so a graph is tuned once.
+For one (graph, k, result limit) it times short enumerations and keeps the
+fastest setting, by coordinate descent from the defaults (each knob in turn
+over its values, the others fixed; `passes` rounds):
+  * warps        resident search warps as a fraction of the occupancy limit
+                 (the block-size / occupancy choice: one-warp blocks, fewer of
+                 them per SM);
+  * hash_load    the edge hash's maximum load in percent (its capacity:
+                 gmk_graph_set_hash_load);
+  * bits_min     k >= 2: the intersection strategy by list length -- candidate
+                 lists of at least this many entries are filtered by bitmaps,
+                 shorter ones by edge-hash probes (0xFFFFFFFF: probes only);
+  * bucket_scale per root-degree bucket b = floor(log32 deg) (the reference's
+                 32^b groups, include/partition.cuh:1136-1190): a factor on the
+                 roots' costs, so that bucket's roots are cut into more (or
+                 fewer) tasks by the planner -- the chunk size per bucket;
+  * tasks_per_worker, donate_min_nodes, pair_limit: the planner's task count,
+                 the in-launch sharing threshold, the node-rule threshold.
+None of them changes the result set.  Winners are cached in a JSON file keyed
+by graph fingerprint, k and limit, so a graph is tuned once.
 """
 from __future__ import annotations
 
@@ -16,28 +26,63 @@ import json
 import os
 import time
 
+import numpy as np
+
 from .api import Graph
 
-DEFAULT_GRID = [
-    dict(chunk=0, split_min_nodes=64, pair_limit=4096),
-    dict(chunk=0, split_min_nodes=16, pair_limit=4096),
-    dict(chunk=0, split_min_nodes=512, pair_limit=4096),
-    dict(chunk=64, split_min_nodes=64, pair_limit=4096),
-    dict(chunk=4096, split_min_nodes=64, pair_limit=4096),
-    dict(chunk=0, split_min_nodes=64, pair_limit=1024),
-    dict(chunk=0, split_min_nodes=64, pair_limit=16384),
-]
+NONE = 0xFFFFFFFF
+DEFAULTS = dict(warps=1.0, hash_load=50, bits_min=64, bucket_scale=(1.0, 1.0, 1.0),
+                tasks_per_worker=8, donate_min_nodes=16, pair_limit=4096)
+CHOICES = {
+    "warps": [0.5, 0.75, 1.0],
+    "hash_load": [25, 50, 90],
+    "bits_min": [32, 64, 256, NONE],
+    "bucket_scale": [(1.0, 1.0, 1.0), (1.0, 2.0, 4.0), (1.0, 4.0, 16.0), (2.0, 1.0, 1.0),
+                     (0.5, 1.0, 2.0)],
+    "tasks_per_worker": [2, 8, 32],
+    "donate_min_nodes": [4, 16, 64],
+    "pair_limit": [1024, 4096, 16384],
+}
+
+
+def degree_buckets(g_host, n_left: int) -> np.ndarray:
+    """floor(log32 deg) of every root, capped at 2 (the root's degree bucket)."""
+    deg = np.diff(np.asarray(g_host.offsets[: n_left + 1], dtype=np.int64))
+    b = np.zeros(n_left, np.int64)
+    b[deg > 32] = 1
+    b[deg > 1024] = 2
+    return b
+
+
+def scaled_costs(base: np.ndarray, buckets: np.ndarray, scale) -> np.ndarray:
+    return (base * np.asarray(scale, np.float64)[buckets]).astype(np.float32)
 
 
 def _key(g: Graph, k: int, limit: int) -> str:
     return f"{g.fingerprint():016x}:k{k}:r{limit}"
 
 
-def tune(g: Graph, k: int, result_limit: int = 200_000, grid=None, repeats: int = 2,
-         cache_path: str | None = None) -> dict:
+def apply(g: Graph, settings: dict, base_cost: np.ndarray, buckets: np.ndarray,
+          max_threads: int) -> dict:
+    """enumerate() keyword arguments for `settings` (and the hash load, set on g)."""
+    g.set_hash_load(int(settings["hash_load"]))
+    warps = max(1, int(max_threads // 32 * settings["warps"]))
+    return dict(schedule="ordered", task_cost=scaled_costs(base_cost, buckets,
+                                                            settings["bucket_scale"]),
+                threads=warps * 32, bits_min_list=int(settings["bits_min"]),
+                tasks_per_worker=int(settings["tasks_per_worker"]),
+                donate_min_nodes=int(settings["donate_min_nodes"]),
+                pair_limit=int(settings["pair_limit"]))
+
+
+def tune(g: Graph, g_host, k: int, base_cost: np.ndarray, result_limit: int = 0,
+         repeats: int = 2, passes: int = 1, cache_path: str | None = None,
+         knobs=None) -> dict:
     """Best settings for enumerating g at k (device time per result, lower is
-    better).  Returns {"settings": {...}, "ms": best_ms, "results": count,
-    "cached": bool, "trials": [...]}."""
+    better), starting from DEFAULTS.  g_host: the graphgen.Graph of g (for the
+    degree buckets); base_cost: per-root costs (the model's prediction or
+    gmk_root_costs).  Returns {"settings", "ms", "default_ms", "gain",
+    "results", "cached", "trials"}."""
     cache_path = cache_path or os.environ.get("GMK_AUTOTUNE_CACHE")
     key = _key(g, k, result_limit)
     cache = {}
@@ -45,20 +90,41 @@ def tune(g: Graph, k: int, result_limit: int = 200_000, grid=None, repeats: int 
         with open(cache_path) as f:
             cache = json.load(f)
         if key in cache:
-            return dict(cache[key], cached=True)
+            out = dict(cache[key], cached=True)
+            out["settings"]["bucket_scale"] = tuple(out["settings"]["bucket_scale"])
+            return out
+    buckets = degree_buckets(g_host, g.n_left)
+    max_threads = g.enumerate(k=k, result_limit=max(1, min(result_limit or 1000, 1000))).threads
     trials = []
-    for s in grid or DEFAULT_GRID:
-        ms = []
-        count = 0
-        for _ in range(repeats):
-            st = g.enumerate(k=k, result_limit=result_limit, schedule="batched", **s)
+
+    def run(settings):
+        kw = apply(g, settings, base_cost, buckets, max_threads)
+        ms, count = [], 0
+        for _ in range(repeats + 1):
+            st = g.enumerate(k=k, result_limit=result_limit, **kw)
             ms.append(st.kernel_ms)
             count = st.count
-        # per result: a setting that stops early on fewer results is not better
-        trials.append({"settings": s, "ms": min(ms), "results": count,
-                       "ms_per_result": min(ms) / max(1, count)})
-    best = min(trials, key=lambda t: t["ms_per_result"])
-    out = {"settings": best["settings"], "ms": best["ms"], "results": best["results"],
+        best = min(ms[1:])
+        trials.append({"settings": dict(settings), "ms": best, "results": count})
+        return best / max(1, count), best, count
+
+    best_s = dict(DEFAULTS)
+    best_v, default_ms, results = run(best_s)
+    for _ in range(passes):
+        for knob in knobs or CHOICES:
+            if knob == "bits_min" and k < 2:
+                continue
+            for val in CHOICES[knob]:
+                if val == best_s[knob]:
+                    continue
+                s = dict(best_s, **{knob: val})
+                v, _, _ = run(s)
+                if v < best_v * 0.98:          # 2 %: below the run-to-run noise
+                    best_v, best_s = v, s
+    g.set_hash_load(int(best_s["hash_load"]))
+    best_ms = best_v * max(1, results)
+    out = {"settings": best_s, "ms": best_ms, "default_ms": default_ms,
+           "gain": default_ms / best_ms if best_ms else None, "results": results,
            "trials": trials, "tuned_at": time.time()}
     if cache_path:
         cache[key] = out

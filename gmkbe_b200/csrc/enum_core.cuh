@@ -146,6 +146,8 @@ struct Outputs {
     unsigned long long out_cap;     // words
     unsigned long long deadline_ns; // 0 = none; compared with the device's global timer
     unsigned long long* out_fail;   // warp engine: lowest record position that found no room
+    int* gstop;                     // warp engine, batches: this graph's limit was reached
+                                    //   (null: the limit raises `stop`)
 };
 
 struct Task {

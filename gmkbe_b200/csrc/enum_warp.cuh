@@ -43,7 +43,8 @@ constexpr uint32_t FL_BITS0 = 32u;        // frame flags: filter bitmaps of list
 constexpr uint32_t FL_BITS1 = 64u;        //   follow the frame's lists (add_filter_bits)
 constexpr uint32_t FL_ONE_PHASE = 128u;   // frame flag: iterate the current phase only (a
                                           //   donated range of its first side's children)
-constexpr uint32_t kBitsMinList = 64;     // shorter lists filter their children by probing
+constexpr uint32_t kBitsMinList = 64;     // default: shorter lists filter their children by
+                                          //   probing (gmk_opts.bits_min_list)
 constexpr uint32_t kBitsMaxZ = 8;         // bitmaps for at most this many members
 constexpr unsigned long long kEmptyKey = ~0ull;
 
@@ -233,6 +234,7 @@ struct Ctx {
     uint32_t ns;
     U2 nss;                                      // |S| per side
     uint32_t scan_limit;
+    uint32_t bits_min;     // k >= 2: lists of at least this many entries get filter bitmaps
     int err;
     unsigned long long cnt, hsum, hxor, nodes;   // warp-uniform
     unsigned long long work;                     // per-lane share
@@ -256,7 +258,7 @@ __device__ void flush(Ctx& t, const Outputs& o) {
             const unsigned long long before = atomicAdd(o.count, t.cnt);
             atomicAdd(o.hash_sum, t.hsum);
             atomicXor(o.hash_xor, t.hxor);
-            if (o.limit && before + t.cnt >= o.limit) atomicExch(o.stop, 1);
+            if (o.limit && before + t.cnt >= o.limit) atomicExch(o.gstop ? o.gstop : o.stop, 1);
         }
         if (t.nodes) atomicAdd(o.nodes, t.nodes);
         if (work) atomicAdd(o.work, work);
@@ -265,6 +267,12 @@ __device__ void flush(Ctx& t, const Outputs& o) {
     t.work = 0;
     __syncwarp();
 }
+
+// A child or a node's scratch did not fit the arena.  Not an error yet: the
+// search loop moves the path into the next round's task list, where each
+// frame restarts at the bottom of an empty arena (run_dfs).
+constexpr int TASK_ARENA_FULL = 99;
+__device__ __forceinline__ void arena_full(Ctx& t) { t.err = TASK_ARENA_FULL; }
 
 __device__ void fail(Ctx& t, const Outputs& o, int code) {
     if (!t.err) t.err = code;
@@ -781,7 +789,7 @@ __device__ __forceinline__ void append_pair(Ctx& t, uint32_t w, uint32_t& cnt, b
 // candidate kept on c's side.  sat(c) lies in Z, the other side's members at
 // k - 1 misses in the frame.  For a long list that adjacency test repeats for
 // every child (O(n^2) probes per frame), so a frame that branches on a list
-// of kBitsMinList or more entries gets one bitmap per member of Z (up to
+// of bits_min (kBitsMinList by default) or more entries gets one bitmap per member of Z (up to
 // kBitsMaxZ): bit q = list entry q is adjacent to z.  Layout, right after the
 // frame's lists (list 0's region first when both exist):
 //   [nz, z_0 .. z_nz-1, end_0 .. end_nz-1,
@@ -804,7 +812,7 @@ __device__ __forceinline__ void add_filter_bits(Ctx& t, uint32_t cur, const Hdr&
     #pragma unroll 1
     for (int s = 0; s < 2; ++s) {
         const uint32_t n = f.cnt.get(s);
-        if ((f.flags & gbit(s)) || n < kBitsMinList) continue;
+        if ((f.flags & gbit(s)) || n < t.bits_min) continue;
         const int o = 1 - s;
         // Z: members of side o at k - 1 misses, in S order
         uint32_t nz = 0;
@@ -865,7 +873,7 @@ __device__ uint32_t build_child(Ctx& t, const Outputs& o, uint32_t cur, uint32_t
     const int os = 1 - s;
     const uint32_t nc = f.top;
     uint32_t w = nc + F_WORDS;
-    if (w > t.cap) { fail(t, o, TASK_E_ARENA); return kNoPos; }
+    if (w > t.cap) { arena_full(t); return kNoPos; }
     Hdr ch;
     ch.ns = t.ns; ch.flags = 0; ch.lo.a = ch.lo.b = 0; ch.cnt.a = ch.cnt.b = 0; ch.off.a = ch.off.b = 0;
     ch.order = 0; ch.phase = 0; ch.pos = 0; ch.parent = cur; ch.end = 0xFFFFFFFFu;
@@ -883,7 +891,7 @@ __device__ uint32_t build_child(Ctx& t, const Outputs& o, uint32_t cur, uint32_t
             for (uint32_t i = 1; i < nsat; ++i)
                 if (degree(g, t.sat[i]) < degree(g, z)) z = t.sat[i];
             const uint32_t dz = degree(g, z);
-            if (w + 2ull * dz > t.cap) { fail(t, o, TASK_E_ARENA); return kNoPos; }
+            if (w + 2ull * dz > t.cap) { arena_full(t); return kNoPos; }
             if (t.lane == 0) t.work += dz;
             const uint32_t* row = g.adj + g.off[z];
             #pragma unroll 1
@@ -904,7 +912,7 @@ __device__ uint32_t build_child(Ctx& t, const Outputs& o, uint32_t cur, uint32_t
     } else {
         const uint32_t* lst = t.arena + f.off.get(s);
         const uint32_t n = f.cnt.get(s);
-        if (w + 2ull * n > t.cap) { fail(t, o, TASK_E_ARENA); return kNoPos; }
+        if (w + 2ull * n > t.cap) { arena_full(t); return kNoPos; }
         const uint32_t start = forced ? 0u : p + 1;
         // the frame's filter bitmaps, when it has them: sel = the rows of sat(c)
         const uint32_t* bm = nullptr;
@@ -1003,7 +1011,7 @@ __device__ uint32_t build_child(Ctx& t, const Outputs& o, uint32_t cur, uint32_t
             unsigned long long bound = 0;
             #pragma unroll 1
             for (uint32_t q = 0; q < nsrc; ++q) bound += degree(g, t.src[q]);
-            if (w + 2 * bound > t.cap) { fail(t, o, TASK_E_ARENA); return kNoPos; }
+            if (w + 2 * bound > t.cap) { arena_full(t); return kNoPos; }
             #pragma unroll 1
             for (uint32_t q = 0; q < nsrc; ++q) {
                 const uint32_t m = t.src[q];
@@ -1034,7 +1042,7 @@ __device__ uint32_t build_child(Ctx& t, const Outputs& o, uint32_t cur, uint32_t
     } else {
         const uint32_t* lst = t.arena + f.off.get(os);
         const uint32_t n = f.cnt.get(os);
-        if (w + 2ull * n > t.cap) { fail(t, o, TASK_E_ARENA); return kNoPos; }
+        if (w + 2ull * n > t.cap) { arena_full(t); return kNoPos; }
         #pragma unroll 1
         for (uint32_t base = 0; base < n; base += 32) {
             const uint32_t q = base + t.lane;
@@ -1087,7 +1095,7 @@ __device__ int enter_node(Ctx& t, const Outputs& o, uint32_t cur, ChildReq* req)
         const int s = g0 ? 0 : 1, os = 1 - s;
         const uint32_t n = f.cnt.get(os);
         const uint32_t base = f.top;
-        if (base + n + 2ull * t.ns > t.cap) { fail(t, o, TASK_E_ARENA); return ENTER_DONE; }
+        if (base + n + 2ull * t.ns > t.cap) { arena_full(t); return ENTER_DONE; }
         if (outsider_addable_mixed(t, s, f.lo.get(s), t.arena + f.off.get(os), n, t.arena + base))
             return ENTER_DONE;
     }
@@ -1099,7 +1107,7 @@ __device__ int enter_node(Ctx& t, const Outputs& o, uint32_t cur, ChildReq* req)
         if (n0 + n1 == 0 || pairs <= t.scan_limit) {
             const uint32_t base = f.top;
             if (base + (unsigned long long)t.ns + n0 + n1 > t.cap) {
-                fail(t, o, TASK_E_ARENA);
+                arena_full(t);
                 return ENTER_DONE;
             }
             uint32_t* tot = t.arena + base;
@@ -1223,7 +1231,7 @@ __device__ int enter_node(Ctx& t, const Outputs& o, uint32_t cur, ChildReq* req)
         fw[F_POS] = (f.flags & gbit((int)order)) ? f.lo.get(order) + 1 : 0;
     }
     __syncwarp();
-    if (kBits && ((!g0 && f.cnt.a >= kBitsMinList) || (!g1 && f.cnt.b >= kBitsMinList)))
+    if (kBits && ((!g0 && f.cnt.a >= t.bits_min) || (!g1 && f.cnt.b >= t.bits_min)))
         add_filter_bits(t, cur, f);
     return ENTER_ITERATE;
 }
@@ -1588,7 +1596,7 @@ __device__ __forceinline__ unsigned long long run_dfs(Ctx& t, const Outputs& o, 
         if ((++polls & GMK_POLL_MASK) == 0) {
             int stop = 0, late = 0, hungry = 0, give = 0;
             if (t.lane == 0) {
-                stop = load_flag(o.stop);
+                stop = load_flag(o.stop) || (o.gstop && load_flag(o.gstop));
                 late = o.deadline_ns && now_ns() > o.deadline_ns;
                 // in-launch sharing while its buffer has room; splitting into
                 // the next round otherwise
@@ -1623,6 +1631,14 @@ __device__ __forceinline__ unsigned long long run_dfs(Ctx& t, const Outputs& o, 
             t.nodes++;
             task_nodes++;
             const int r = enter_node<kRec, kBits>(t, o, cur, &req);
+            if (t.err == TASK_ARENA_FULL) {
+                // the node's scratch did not fit: it is entered again next
+                // round, from the bottom of an empty arena (after the loop)
+                if (t.lane == 0) f[F_FLAGS] &= ~FL_ENTERED;
+                __syncwarp();
+                t.nodes--;
+                break;
+            }
             if (kRec && r == ENTER_DEFER) {
                 // re-enter this node next round, after the host drained the buffer
                 set_word(t, cur + F_FLAGS, flags);
@@ -1644,7 +1660,26 @@ __device__ __forceinline__ unsigned long long run_dfs(Ctx& t, const Outputs& o, 
         if (!want) want = next_child(t, cur, &req);
         if (!want) { cur = f[F_PARENT_SLOT]; continue; }
         const uint32_t ch = build_child<kBits>(t, o, cur, req.c, req.s, req.p, req.forced, req.opp_done);
+        if (t.err == TASK_ARENA_FULL) {
+            // the child did not fit: put the frame back where it was before
+            // this child -- a forced child (phase 2) re-enters the node, any
+            // other steps back one position in its phase -- and move the path
+            // to the next round, where each frame starts an empty arena.  A
+            // task's base frame that cannot fit one child is a real overflow.
+            if (t.lane == 0) {
+                if (f[F_PHASE] == 2) f[F_FLAGS] &= ~FL_ENTERED;
+                else f[F_POS] -= 1;
+            }
+            __syncwarp();
+            break;
+        }
         cur = ch == kNoPos ? f[F_PARENT_SLOT] : ch;   // kNoPos: t.err is set, the loop ends
+    }
+    if (t.err == TASK_ARENA_FULL) {
+        // the path moves to the next round; only a task's base frame that
+        // cannot hold its own node or one child is an arena overflow
+        t.err = 0;
+        if (!(cur != 0 && sb && split_path(t, *sb, cur))) fail(t, o, TASK_E_ARENA);
     }
     pop_to(t, 0);
     return task_nodes;

@@ -67,6 +67,8 @@ struct RoundCounters {
 };
 
 constexpr int kBlock = 128;
+// Edge hash: at most this percentage of its slots hold keys (two per bucket of four).
+constexpr uint32_t kDefaultHashLoad = 50;
 constexpr uint32_t kDefaultArena = 1u << 16;
 constexpr uint32_t kDefaultSmax = 2048;
 // Node rules run while |S u C_U| x |S u C_V| is at most this (gmk_opts.pair_limit 0).
@@ -93,6 +95,7 @@ enumerate_kernel(gmk::GraphView g, uint32_t k, Counters* ctr, uint32_t* arenas,
     o.nodes = &ctr->nodes; o.work = &ctr->work; o.stop = &ctr->stop; o.error = &ctr->error;
     o.limit = limit; o.out_buf = out_buf; o.out_pos = &ctr->out_pos; o.out_cap = out_cap;
     o.out_fail = nullptr;
+    o.gstop = nullptr;
     o.deadline_ns = watchdog_ns ? gmk::now_ns() + watchdog_ns : 0ull;
     gmk::Task t;
     t.g = g; t.k = k;
@@ -161,6 +164,7 @@ struct GraphTask {
     gmk::warp::EdgeHash eh;
     uint32_t k;
     uint32_t chunk, n_roots, root_base;
+    unsigned long long limit;          // batches: this graph's result cap (0: none)
     Counters* ctr;                     // counts, hashes, nodes, work of this graph
     unsigned long long* root_nodes;    // optional per-root node log
     unsigned long long task_begin;
@@ -177,6 +181,7 @@ struct WarpArgs {
     uint32_t* sbuf;
     uint32_t smax;
     uint32_t pair_limit;
+    uint32_t bits_min_list;            // k >= 2: filter bitmaps for lists this long
     // the round's queue: entries [0, n_records) are split records, the rest
     // root tasks root_task_base, root_task_base + 1, ... (this shard's numbering)
     unsigned long long n_records;
@@ -214,6 +219,11 @@ __device__ __forceinline__ const GraphTask& use_graph(const WarpArgs& a, uint32_
     t.gid = gid;
     o.count = &G.ctr->count; o.hash_sum = &G.ctr->hash_sum; o.hash_xor = &G.ctr->hash_xor;
     o.nodes = &G.ctr->nodes; o.work = &G.ctr->work;
+    if (kBatch) {
+        // each graph of a batch has its own cap; reaching it stops that graph only
+        o.limit = G.limit;
+        o.gstop = &G.ctr->stop;
+    }
     return G;
 }
 
@@ -234,6 +244,7 @@ enumerate_warp_kernel(const __grid_constant__ WarpArgs a) {
     o.nodes = &ctr->nodes; o.work = &ctr->work; o.stop = &ctr->stop; o.error = &ctr->error;
     o.limit = a.limit; o.out_buf = a.out_buf; o.out_pos = &a.rc->out_pos; o.out_cap = a.out_cap;
     o.out_fail = &a.rc->out_fail;
+    o.gstop = nullptr;
     o.deadline_ns = 0;
     if (a.watchdog_ns) {
         // the first warp of the first round fixes the origin of the watchdog
@@ -252,6 +263,7 @@ enumerate_warp_kernel(const __grid_constant__ WarpArgs a) {
     t.smax = a.smax; t.mask_base = 0;
     t.ns = 0; t.nss.a = t.nss.b = 0;
     t.scan_limit = a.pair_limit; t.err = 0;
+    t.bits_min = a.bits_min_list;
     t.cnt = t.hsum = t.hxor = t.nodes = 0; t.work = 0;
     t.sat = s_sat[wib]; t.src = s_src[wib]; t.lane = lane;
     RunLimits lim;
@@ -260,7 +272,9 @@ enumerate_warp_kernel(const __grid_constant__ WarpArgs a) {
     lim.queue_len = a.queue_len;
     lim.out_pos = &a.rc->out_pos;
     lim.drain_at = a.drain_at;
-    const SplitBuf* sb = (a.split_min_nodes || a.drain_at) ? &a.next : nullptr;
+    // the next round's task list: load balance and record draining split into
+    // it, and so does any path that outgrows the arena (plain schedule too)
+    const SplitBuf* sb = &a.next;
     const Donation* db = (!kRec && a.share.words) ? &a.share : nullptr;
     for (;;) {
         unsigned long long j = ~0ull;
@@ -378,8 +392,10 @@ enumerate_warp_kernel(const __grid_constant__ WarpArgs a) {
                 const unsigned long long end = (unsigned long long)first + G.chunk;
                 last = end < t.g.n ? (uint32_t)end : t.g.n;
             }
-            const unsigned long long nodes = run_root<kRec, kBits>(t, o, root, first, last, sb, lim, db);
-            if (G.root_nodes && lane == 0) atomicAdd(G.root_nodes + root, nodes);
+            if (!(kBatch && gmk::load_flag(o.gstop))) {   // a capped graph's tasks end at once
+                const unsigned long long nodes = run_root<kRec, kBits>(t, o, root, first, last, sb, lim, db);
+                if (G.root_nodes && lane == 0) atomicAdd(G.root_nodes + root, nodes);
+            }
         }
         if (db && lane == 0) atomicAdd(db->outstanding, ~0ull);   // this task is finished
         flush(t, o);
@@ -466,6 +482,8 @@ struct gmk_graph {
     unsigned long long* d_eh = nullptr;   // edge hash: buckets of 4 keys
     unsigned long long eh_bmask = 0;
     size_t eh_bytes = 0;
+    unsigned long long u_edges = 0;       // |E| (entries of the U rows)
+    uint32_t hash_load = 0;               // the edge hash's maximum load, percent
     unsigned long long* d_root_nodes = nullptr;   // per-root node log (on demand)
     __half* d_feat = nullptr;                     // root features (on demand)
     float* d_cost = nullptr;                      // root cost proxy (on demand)
@@ -492,6 +510,8 @@ struct Workspace {
     uint32_t* d_out = nullptr;
     size_t out_bytes = 0;
     void* d_graphs = nullptr;     // the launch's GraphTask array
+    Counters* d_launch = nullptr; // batches: the launch's own stop / error / watchdog words
+    size_t launch_bytes = 0;
     size_t graphs_bytes = 0;
     // two split buffers (this round's records, the next round's)
     uint32_t* d_split_words[2] = {nullptr, nullptr};
@@ -608,6 +628,28 @@ void pool_return(int dev, cudaStream_t s, cudaEvent_t ev) {
 int deliver_records(gmk_graph* g, const uint32_t* d_rec, unsigned long long words, gmk_sink sink,
                     void* user);
 
+// Edge hash of g at a maximum load of load_pct percent of its slots (buckets
+// of four 8-byte keys, a power of two of them); replaces any earlier one.
+int build_hash(gmk_graph* g, uint32_t load_pct) {
+    const unsigned long long edges = g->u_edges;
+    unsigned long long buckets = 1;
+    while (buckets * 4ull * load_pct < edges * 100ull) buckets <<= 1;
+    if (g->d_eh) pool_free(g->device, g->d_eh, g->eh_bytes);
+    g->d_eh = nullptr;
+    g->eh_bmask = buckets - 1;
+    g->eh_bytes = buckets * 4 * sizeof(unsigned long long);
+    g->hash_load = load_pct;
+    CK(pool_alloc(g->device, (void**)&g->d_eh, g->eh_bytes));
+    CK(cudaMemsetAsync(g->d_eh, 0xFF, g->eh_bytes, g->stream));
+    if (edges) {
+        const unsigned grid = (unsigned)((edges + 255) / 256);
+        gmk::warp::build_edge_hash<<<grid, 256, 0, g->stream>>>(g->d_off, g->d_adj, g->nl, g->d_eh,
+                                                                 g->eh_bmask);
+        CK(cudaGetLastError());
+    }
+    return GMK_OK;
+}
+
 int upload(const uint32_t* off, const uint32_t* adj, uint32_t n, uint32_t nl, int device,
            gmk_graph** out) {
     if (nl > n || off[0] != 0) return GMK_E_FORMAT;
@@ -666,26 +708,8 @@ int upload(const uint32_t* off, const uint32_t* adj, uint32_t n, uint32_t nl, in
         if (hc.bad) return bail(GMK_E_FORMAT);
         g->fingerprint = gmk::mix64(hc.fp ^ (((uint64_t)n << 32) | nl));
     }
-    // edge hash: at most two keys per four slots
-    {
-        const unsigned long long edges = off[nl];
-        unsigned long long buckets = 1;
-        while (buckets * 2 < edges) buckets <<= 1;
-        g->eh_bmask = buckets - 1;
-        const size_t bytes = buckets * 4 * sizeof(unsigned long long);
-        g->eh_bytes = bytes;
-        if ((e = pool_alloc(device, (void**)&g->d_eh, bytes)) != cudaSuccess)
-            return bail(cuda_fail(e, "cudaMalloc(edge hash)"));
-        if ((e = cudaMemsetAsync(g->d_eh, 0xFF, bytes, g->stream)) != cudaSuccess)
-            return bail(cuda_fail(e, "memset(edge hash)"));
-        if (edges) {
-            const unsigned grid = (unsigned)((edges + 255) / 256);
-            gmk::warp::build_edge_hash<<<grid, 256, 0, g->stream>>>(g->d_off, g->d_adj, nl, g->d_eh,
-                                                                     g->eh_bmask);
-            if ((e = cudaGetLastError()) != cudaSuccess)
-                return bail(cuda_fail(e, "build_edge_hash"));
-        }
-    }
+    g->u_edges = off[nl];
+    if (int rc = build_hash(g, kDefaultHashLoad)) return bail(rc);
     if ((e = cudaStreamSynchronize(g->stream)) != cudaSuccess) return bail(cuda_fail(e, "upload"));
     *out = g;
     return GMK_OK;
@@ -798,6 +822,15 @@ int gmk_graph_info(const gmk_graph* g, uint32_t* n, uint32_t* n_left, uint64_t* 
     return GMK_OK;
 }
 
+int gmk_graph_set_hash_load(gmk_graph* g, uint32_t load_pct) {
+    if (!g || load_pct < 10 || load_pct > 100) return GMK_E_INVAL;
+    CK(cudaSetDevice(g->device));
+    if (load_pct == g->hash_load) return GMK_OK;
+    if (int rc = build_hash(g, load_pct)) return rc;
+    CK(cudaStreamSynchronize(g->stream));
+    return GMK_OK;
+}
+
 int gmk_graph_fingerprint(const gmk_graph* g, uint64_t* out) {
     if (!g || !out) return GMK_E_INVAL;
     *out = g->fingerprint;
@@ -907,6 +940,7 @@ void order_and_shard(std::vector<gmk_task>& tasks, uint32_t nshards, uint32_t sh
 struct GraphJob {
     gmk_graph* g;
     uint32_t k;
+    uint64_t limit;               // batches: the graph's result cap (0: none)
     uint32_t root_begin, root_end;
     const float* task_cost;       // ORDERED schedule: one cost per root
     uint64_t* root_nodes;         // optional host log
@@ -998,6 +1032,7 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
     std::vector<uint32_t> chunks(ng), cprs(ng);
     const uint32_t nsh = opts->nshards > 1 ? opts->nshards : 1u;
     const uint32_t sh = nsh > 1 ? opts->shard : 0u;
+    const uint32_t tasks_per = opts->tasks_per_worker ? opts->tasks_per_worker : 8u;
     // (a plain run given costs keeps one task per root and no splitting, but
     // starts the largest predicted roots first: the static schedule with the
     // learned order)
@@ -1020,7 +1055,7 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
             for (const uint32_t r : roots[i]) total += std::max<double>(costs[i][r], 0.0);
         }
         const uint32_t max_chunks = opts->schedule == GMK_SCHEDULE_PLAIN ? 1u : 0xFFFFFFFFu;
-        const double unit = total / (double)std::max<uint64_t>(1, 8ull * workers);
+        const double unit = total / (double)std::max<uint64_t>(1, (uint64_t)tasks_per * workers);
         for (size_t i = 0; i < ng; ++i)
             chunk_roots(jobs[i].g->nl, jobs[i].g->n, roots[i], costs[i], unit, max_chunks,
                         (uint32_t)i, plan);
@@ -1037,8 +1072,8 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
             if (opts->chunk) {
                 chunk = std::min(opts->chunk, nv);
             } else {
-                // about 8 tasks per worker, but no chunk below 16 children
-                const uint64_t want = 8ull * workers;
+                // about tasks_per (8) tasks per worker, but no chunk below 16 children
+                const uint64_t want = (uint64_t)tasks_per * workers;
                 const uint64_t per_root = (want + g->nl - 1) / std::max<uint32_t>(g->nl, 1);
                 chunk = (uint32_t)std::max<uint64_t>(16, (nv + per_root - 1) / std::max<uint64_t>(1, per_root));
                 chunk = std::min(chunk, nv);
@@ -1054,6 +1089,7 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
         t.chunk = chunk;
         t.n_roots = nroots;
         t.root_base = j.root_begin;
+        t.limit = j.limit;
         t.ctr = g->d_ctr;
         t.root_nodes = nullptr;
         if (j.root_nodes) {
@@ -1126,7 +1162,16 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
     const unsigned grid = (unsigned)(threads / block);
     const unsigned long long watchdog_ns = (unsigned long long)opts->watchdog_ms * 1000000ull;
     const uint32_t pair_limit = opts->pair_limit ? opts->pair_limit : kDefaultPairLimit;
-    Counters h;          // launch-wide flags (graph 0's counters)
+    // launch-wide flags: graph 0's counters for one graph; a batch has its own
+    // block, since each graph's `stop` there means "this graph reached its cap"
+    Counters* launch_ctr = g0->d_ctr;
+    if (ng > 1) {
+        if ((rc = grow((void**)&ws.d_launch, &ws.launch_bytes, sizeof(Counters)))) return rc;
+        CK(cudaMemsetAsync(ws.d_launch, 0, sizeof(Counters), g0->stream));
+        launch_ctr = ws.d_launch;
+    }
+    const unsigned long long single_limit = opts->result_limit ? opts->result_limit : jobs[0].limit;
+    Counters h;          // launch-wide flags
     unsigned long long tasks_total = 0, tasks_done = 0, donations = 0;
     uint32_t rounds = 0;
     int warp_emit_rc = GMK_OK;
@@ -1149,15 +1194,16 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
         a.single = gt[0];
         a.graphs = static_cast<const GraphTask*>(ws.d_graphs);
         a.n_graphs = (uint32_t)ng;
-        a.ctr = g0->d_ctr;
+        a.ctr = launch_ctr;
         a.rc = g0->d_rc;
         a.arenas = ws.d_arena;
         a.arena_words = arena_words;
         a.sbuf = ws.d_sbuf;
         a.smax = smax;
         a.pair_limit = pair_limit;
+        a.bits_min_list = opts->bits_min_list ? opts->bits_min_list : gmk::warp::kBitsMinList;
         a.split_min_nodes = split_min;
-        a.limit = opts->result_limit;
+        a.limit = single_limit;
         a.out_buf = opts->emit ? ws.d_out : nullptr;
         a.out_cap = out_words;
         a.watchdog_ns = watchdog_ns;
@@ -1230,7 +1276,7 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
             }
             RoundCounters r;
             CK(cudaMemcpyAsync(&r, g0->d_rc, sizeof(r), cudaMemcpyDeviceToHost, g0->stream));
-            CK(cudaMemcpyAsync(&h, g0->d_ctr, sizeof(h), cudaMemcpyDeviceToHost, g0->stream));
+            CK(cudaMemcpyAsync(&h, launch_ctr, sizeof(h), cudaMemcpyDeviceToHost, g0->stream));
             CK(cudaStreamSynchronize(g0->stream));
             ++rounds;
             tasks_total += a.queue_len;
@@ -1281,10 +1327,10 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
     CK(cudaEventElapsedTime(&ms, g0->ev0, g0->ev1));
     for (size_t i = 0; i < ng; ++i) {
         Counters hc = h;
-        if (i) CK(cudaMemcpy(&hc, jobs[i].g->d_ctr, sizeof(hc), cudaMemcpyDeviceToHost));
+        if (ng > 1) CK(cudaMemcpy(&hc, jobs[i].g->d_ctr, sizeof(hc), cudaMemcpyDeviceToHost));
         gmk_stats* out = outs + i;
-        out->count = opts->result_limit ? std::min<unsigned long long>(hc.count, opts->result_limit)
-                                        : hc.count;
+        const unsigned long long cap = ng > 1 ? jobs[i].limit : single_limit;
+        out->count = cap ? std::min<unsigned long long>(hc.count, cap) : hc.count;
         out->hash_sum = hc.hash_sum;
         out->hash_xor = hc.hash_xor;
         out->nodes = hc.nodes;
@@ -1292,7 +1338,7 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
         out->tasks = tasks_total;
         out->tasks_done = tasks_done;
         out->kernel_ms = ms;
-        out->truncated = opts->result_limit && hc.count >= opts->result_limit;
+        out->truncated = cap && hc.count >= cap;
         out->threads = (uint32_t)threads;
         out->rounds = rounds;
         out->donations = donations;
@@ -1385,13 +1431,14 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
     std::memset(out, 0, sizeof(*out));
     CK(cudaSetDevice(g->device));
     if (g->nl == 0 || g->n == g->nl || opts->root_begin == root_end) return GMK_OK;   // nothing to do
-    std::vector<GraphJob> jobs{{g, opts->k, opts->root_begin, root_end, opts->task_cost,
+    std::vector<GraphJob> jobs{{g, opts->k, 0, opts->root_begin, root_end, opts->task_cost,
                                 opts->root_nodes}};
     return run_jobs(jobs, opts, sink, user, out);
 }
 
 int gmk_enumerate_batch(gmk_graph* const* graphs, uint32_t n_graphs, const uint32_t* ks,
-                        const float* const* task_costs, const gmk_opts* opts, gmk_stats* outs) {
+                        const uint64_t* limits, const float* const* task_costs,
+                        const gmk_opts* opts, gmk_stats* outs) {
     if (!graphs || !opts || !outs || n_graphs == 0) return GMK_E_INVAL;
     if (int rc = check_opts(opts)) return rc;
     if (opts->engine != GMK_ENGINE_WARP || opts->emit || opts->result_limit || opts->root_nodes ||
@@ -1410,7 +1457,8 @@ int gmk_enumerate_batch(gmk_graph* const* graphs, uint32_t n_graphs, const uint3
         for (uint32_t j = 0; j < i; ++j)
             if (graphs[j] == g) return GMK_E_INVAL;   // each graph's counters are its own
         if (g->nl == 0 || g->n == g->nl) continue;    // a side is empty: no k-biplex
-        jobs.push_back({g, k, 0, g->nl, task_costs ? task_costs[i] : nullptr, nullptr});
+        jobs.push_back({g, k, limits ? limits[i] : 0ull, 0, g->nl,
+                        task_costs ? task_costs[i] : nullptr, nullptr});
         slot.push_back(i);
     }
     if (jobs.empty()) return GMK_OK;

@@ -62,6 +62,15 @@ int gmk_graph_info(const gmk_graph* g, uint32_t* n, uint32_t* n_left, uint64_t* 
  * caches record. */
 int gmk_graph_fingerprint(const gmk_graph* g, uint64_t* out);
 
+/* No counterpart in the reference (its membership test is a binary search of
+ * sorted rows, include/gpu_utils.cuh:258-282).  Rebuilds the graph's device
+ * edge hash -- the membership structure of every adjacency test -- so that at
+ * most load_pct percent of its slots hold keys (10..100; 50 at load).  A
+ * lower load costs memory and keeps probes inside one 32-byte bucket; a
+ * higher one shrinks the table (fewer L2 misses on large graphs).  The
+ * autotuner picks it per graph. */
+int gmk_graph_set_hash_load(gmk_graph* g, uint32_t load_pct);
+
 /* Releases the graph's device memory (its buffers go to a per-device cache for
  * the next load).  The reference frees its device arrays when the process
  * exits; there is no separate call. */
@@ -126,6 +135,11 @@ typedef struct {
                                  instead of planning; needs nshards <= 1, no root range,
                                  and one graph.  Used to re-run a failed rank's shard. */
     uint64_t n_tasks;         /* entries of tasks */
+    uint32_t tasks_per_worker; /* batched / ordered: root tasks planned per warp; 0 = 8 */
+    uint32_t bits_min_list;   /* warp engine, k >= 2: the intersection strategy by list length --
+                                 a branching node's candidate lists of at least this many entries
+                                 get filter bitmaps (bit tests), shorter ones are filtered by
+                                 edge-hash probes; 0 = 64, 0xFFFFFFFF = probes only */
 } gmk_opts;
 
 typedef struct {
@@ -171,13 +185,17 @@ int gmk_enumerate(gmk_graph* g, const gmk_opts* opts, gmk_sink sink, void* user,
  * n_graphs graphs, all loaded on the same device, in one run of persistent
  * launches: the root tasks of every graph share one device work queue, so
  * many small or uneven graphs keep the GPU busy together.  ks[i] is graph i's
- * k (NULL: opts->k for all); with GMK_SCHEDULE_ORDERED, task_costs[i] gives
- * graph i's per-root costs.  Full enumeration only: opts must have emit = 0,
- * result_limit = 0, no root range, no root_nodes, no sharding, and the warp
- * engine.  outs[i] receives graph i's count and set hash (kernel_ms, rounds
- * and tasks are those of the whole batch).  A graph may appear only once. */
+ * k (NULL: opts->k for all); limits[i] is graph i's result cap (NULL or 0: all
+ * of its results) -- a graph that reaches its cap stops alone, the others go
+ * on; with GMK_SCHEDULE_ORDERED, task_costs[i] gives graph i's per-root costs.
+ * opts must have emit = 0, result_limit = 0, no root range, no root_nodes, no
+ * sharding, no task list, and the warp engine.  outs[i] receives graph i's
+ * count (clamped to its cap, truncated set when reached) and set hash (a set
+ * summary only when not truncated); kernel_ms, rounds and tasks are those of
+ * the whole batch.  A graph may appear only once. */
 int gmk_enumerate_batch(gmk_graph* const* graphs, uint32_t n_graphs, const uint32_t* ks,
-                        const float* const* task_costs, const gmk_opts* opts, gmk_stats* outs);
+                        const uint64_t* limits, const float* const* task_costs,
+                        const gmk_opts* opts, gmk_stats* outs);
 
 /* No counterpart in the reference, which has no resume (its "checkpoints" are
  * result-count milestones, src/main.cu:1753-1761).  Runs gmk_enumerate over

@@ -10,10 +10,12 @@
 // 4 x words / results as the bytes one result costs (the roofline's
 // algorithmic bytes).  The product never runs this file.
 //
-//   work_count <file.graph.bin> <k> [result_limit]
-// prints one JSON line: results, nodes, adjacency_words, algo_bytes.
+//   work_count <file.graph.bin> <k> [result_limit] [--per-root]
+// prints one JSON line: results, nodes, adjacency_words, algo_bytes (and with
+// --per-root the search nodes of every root task, "root_nodes").
 #include <cstdio>
 #include <cstdlib>
+#include <string>
 #include <vector>
 
 #include "../gmkbe_b200/csrc/enum_core.cuh"
@@ -25,6 +27,7 @@ int main(int argc, char** argv) {
     }
     const unsigned k = (unsigned)std::strtoul(argv[2], nullptr, 10);
     const unsigned long long limit = argc > 3 ? std::strtoull(argv[3], nullptr, 10) : 0ull;
+    const bool per_root = argc > 4 && std::string(argv[4]) == "--per-root";
     FILE* fp = std::fopen(argv[1], "rb");
     if (!fp) { std::perror(argv[1]); return 1; }
     std::vector<uint32_t> w;
@@ -69,15 +72,24 @@ int main(int argc, char** argv) {
     t.arena = arena.data(); t.cap = cap;
     t.sid = sid.data(); t.smc = smc.data(); t.smax = smax;
     t.scan_limit = 4096;
+    std::vector<unsigned long long> root_nodes(nl, 0);
     for (uint32_t root = 0; root < nl && !stop; ++root) {
+        const unsigned long long before = nodes + t.nodes;
         gmk::run_task(t, o, root, nl, n);
+        root_nodes[root] = nodes + t.nodes - before;
         gmk::flush(t, o);
         if (t.err) { std::fprintf(stderr, "task error %d at root %u\n", t.err, root); return 1; }
     }
     gmk::flush(t, o);
     std::printf("{\"results\": %llu, \"nodes\": %llu, \"adjacency_words\": %llu, "
                 "\"algo_bytes\": %llu, \"hash_sum\": \"%016llx\", \"hash_xor\": \"%016llx\", "
-                "\"k\": %u, \"result_limit\": %llu}\n",
+                "\"k\": %u, \"result_limit\": %llu",
                 count, nodes, work, 4ull * work, hsum, hxor, k, limit);
+    if (per_root) {
+        std::printf(", \"root_nodes\": [");
+        for (uint32_t r = 0; r < nl; ++r) std::printf(r ? ", %llu" : "%llu", root_nodes[r]);
+        std::printf("]");
+    }
+    std::printf("}\n");
     return 0;
 }

@@ -59,4 +59,43 @@ def test_batch_rejects_unsupported_options():
         with pytest.raises(G.GmkError):
             G.enumerate_batch([dg, dg], [1, 1])        # the same graph twice
         lib = G.load_library()
-        assert lib.gmk_enumerate_batch(None, 0, None, None, None, None) == -1
+        assert lib.gmk_enumerate_batch(None, 0, None, None, None, None, None) == -1
+
+
+def test_per_graph_caps_stop_each_graph_alone():
+    # graph i stops at its own cap; graphs whose full set is below their cap
+    # are enumerated completely and stay bit-exact
+    gs, ks = _batch(16, 500)
+    dgs = [G.Graph.from_graph(g) for g in gs]
+    try:
+        full = [dg.enumerate(k=k, schedule="plain") for dg, k in zip(dgs, ks)]
+        caps = [max(1, f.count // 3) if i % 2 else f.count + 10 for i, f in enumerate(full)]
+        got = G.enumerate_batch(dgs, ks, limits=caps)
+        for f, cap, st in zip(full, caps, got):
+            if cap > f.count:
+                assert st.summary() == f.summary() and not st.truncated
+            else:
+                assert st.count == cap and st.truncated
+    finally:
+        for dg in dgs:
+            dg.close()
+
+
+def test_stated_size_mixed_batch_with_caps():
+    # the mixed batch at its stated sizes (|U|, |V| log-uniform in [1k, 50k],
+    # average degree 5-30, half Erdos-Renyi and half Chung-Lu, k in {1,2,3};
+    # 16 of the 64 seeds): every graph has far more maximal k-biplexes than
+    # the cap, so each must stop at exactly its cap, as its own capped run does
+    gs, ks = gg.mixed_batch(16, 100)
+    cap = 50_000
+    dgs = [G.Graph.from_graph(g) for g in gs]
+    try:
+        got = G.enumerate_batch(dgs, ks, limits=[cap] * len(dgs))
+        for dg, k, st in zip(dgs, ks, got):
+            single = dg.enumerate(k=k, result_limit=cap)
+            assert st.count == single.count
+            assert st.truncated == single.truncated
+        assert sum(st.count for st in got) > 0
+    finally:
+        for dg in dgs:
+            dg.close()

@@ -224,11 +224,29 @@ def test_result_limit_count_mode(graphs):
 
 
 def test_small_arena_reports_error_not_fault(graphs):
+    # the per-thread engine cannot split: an arena too small for its search
+    # is an error; for the warp engine, 20 words cannot hold a task's base
+    # frame and its first child
     with pytest.raises(G.GmkError) as e:
-        graphs("er200").enumerate(k=1, arena_words=40)
+        graphs("er200").enumerate(k=1, arena_words=40, engine="thread")
+    assert e.value.code == -6
+    with pytest.raises(G.GmkError) as e:
+        graphs("er200").enumerate(k=1, arena_words=20)
     assert e.value.code == -6
     # the context stays usable
     assert graphs("er60").enumerate(k=1).count == 8041
+
+
+@pytest.mark.parametrize("schedule,arena", [("batched", 160), ("batched", 400), ("plain", 400)])
+def test_paths_that_outgrow_the_arena_move_to_the_next_round(golden, graphs, schedule, arena):
+    # a child (or a node's scratch) that does not fit sends the task's path to
+    # the next round, each frame at the bottom of an empty arena: the set is
+    # unchanged and only extra rounds show it
+    for name, k in [("er200", 1), ("southernwomen", 2), ("er60", 2)]:
+        case = next(c for c in golden["cases"] if c["graph"] == name and c["k"] == k)
+        st = graphs(name).enumerate(k=k, arena_words=arena, schedule=schedule)
+        assert st.summary() == _summary(case), (name, k, arena)
+        assert st.rounds > 1
 
 
 def test_watchdog_returns_status():
@@ -252,15 +270,42 @@ def test_limited_run_at_full_size():
         assert O.classify(g, 1, x, y) == 2
 
 
-def test_autotuner_picks_a_setting_and_caches_it(tmp_path):
+def test_autotuner_picks_a_setting_and_caches_it(golden, tmp_path):
+    # every knob is tried (k = 2 also tries the intersection strategy); the
+    # winner is cached per fingerprint, and no setting changes the result set
     from gmkbe_b200 import autotune
     cache = str(tmp_path / "tune.json")
-    with G.Graph.load(golden_graph_path("er200")) as g:
-        first = autotune.tune(g, 1, result_limit=20_000, repeats=1, cache_path=cache)
-        assert not first["cached"] and first["results"] == 20_000
+    want = _summary(next(c for c in golden["cases"] if c["graph"] == "er60" and c["k"] == 2))
+    h = gg.read_graph_bin(golden_graph_path("er60"))
+    with G.Graph.from_graph(h) as g:
+        cost = g.root_costs()
+        first = autotune.tune(g, h, 2, cost, repeats=1, cache_path=cache)
+        assert not first["cached"] and first["results"] == want[0]
         assert first["settings"] in [t["settings"] for t in first["trials"]]
-        again = autotune.tune(g, 1, result_limit=20_000, cache_path=cache)
+        tried = {kn for t in first["trials"] for kn, v in t["settings"].items()
+                 if v != autotune.DEFAULTS[kn]}
+        assert tried == set(autotune.CHOICES)
+        again = autotune.tune(g, h, 2, cost, cache_path=cache)
         assert again["cached"] and again["settings"] == first["settings"]
-        # the tuned settings keep the set
-        case_full = g.enumerate(k=1).summary()
-        assert g.enumerate(k=1, **first["settings"]).summary() == case_full
+        buckets = autotune.degree_buckets(h, g.n_left)
+        for t in first["trials"]:
+            kw = autotune.apply(g, t["settings"], cost, buckets, 4144 * 32)
+            assert g.enumerate(k=2, **kw).summary() == want, t["settings"]
+
+
+@pytest.mark.parametrize("load", [10, 25, 90, 100])
+def test_edge_hash_load_keeps_the_set(golden, load):
+    with G.Graph.load(golden_graph_path("crime")) as g:
+        g.set_hash_load(load)
+        st = g.enumerate(k=1)
+    assert st.summary() == _summary(next(c for c in golden["cases"] if c["graph"] == "crime"
+                                         and c["k"] == 1))
+
+
+@pytest.mark.parametrize("bits_min", [1, 2, 32, 0xFFFFFFFF])
+def test_intersection_strategy_keeps_the_set(bits_min):
+    # bitmaps for every list (1), for lists of two or more, or never (probes)
+    g = gg.hubs_and_sparse(4, 60, 150, 3, 7)
+    with G.Graph.from_graph(g) as dg:
+        want = O.enumerate_oracle(g, 2).summary()
+        assert dg.enumerate(k=2, bits_min_list=bits_min).summary() == want

@@ -48,6 +48,12 @@
 #endif
 #endif
 
+// Hook for host-side measurement tools (the arena's high-water mark); empty in
+// the library.
+#ifndef GMK_TRACE_TOP
+#define GMK_TRACE_TOP(task, top) ((void)0)
+#endif
+
 #ifndef GMK_LOCAL_ORDER
 #define GMK_LOCAL_ORDER(n0, n1) ((n1) < (n0) ? 1u : 0u)
 #endif
@@ -594,6 +600,7 @@ GMK_HD uint32_t build_child(Task& t, const Outputs& o, uint32_t cur, uint32_t c,
     ch[F_CNT0 + os] = cnt;
     w += 2 * cnt;
     ch[F_TOP] = w;
+    GMK_TRACE_TOP(t, w);
     normalise(g, ch);
     return nc;
 }

@@ -43,6 +43,9 @@ constexpr uint32_t FL_BITS0 = 32u;        // frame flags: filter bitmaps of list
 constexpr uint32_t FL_BITS1 = 64u;        //   follow the frame's lists (add_filter_bits)
 constexpr uint32_t FL_ONE_PHASE = 128u;   // frame flag: iterate the current phase only (a
                                           //   donated range of its first side's children)
+constexpr uint32_t FL_SHARED0 = 256u;     // frame flags: list 0 / list 1 is a suffix of the
+constexpr uint32_t FL_SHARED1 = 512u;     //   parent's list, read in place (not stored after
+                                          //   the frame)
 constexpr uint32_t kBitsMinList = 64;     // default: shorter lists filter their children by
                                           //   probing (gmk_opts.bits_min_list)
 constexpr uint32_t kBitsMaxZ = 8;         // bitmaps for at most this many members
@@ -798,7 +801,9 @@ __device__ __forceinline__ void append_pair(Ctx& t, uint32_t w, uint32_t& cnt, b
 // whose candidates start past it keeps nothing without reading the bitmap.
 // Split records do not carry them; a restored frame filters by probing.
 __device__ __forceinline__ uint32_t bits_region(const Ctx& t, uint32_t cur, const Hdr& f, int s) {
-    uint32_t at = cur + F_WORDS + 2 * (((f.flags & FL_G0) ? 0u : f.cnt.a) + ((f.flags & FL_G1) ? 0u : f.cnt.b));
+    // after the lists the frame stores itself (global and shared sides store none)
+    uint32_t at = cur + F_WORDS + 2 * (((f.flags & (FL_G0 | FL_SHARED0)) ? 0u : f.cnt.a) +
+                                       ((f.flags & (FL_G1 | FL_SHARED1)) ? 0u : f.cnt.b));
     if (s == 1 && (f.flags & FL_BITS0)) {
         const uint32_t nz0 = t.arena[at];
         at += 1 + 2 * nz0 + nz0 * ((f.cnt.a + 31) >> 5);
@@ -909,6 +914,14 @@ __device__ uint32_t build_child(Ctx& t, const Outputs& o, uint32_t cur, uint32_t
                 append_pair(t, w, cnt, keep, v, m);
             }
         }
+    } else if (!forced && nsat == 0) {
+        // nothing to filter: the child's list is the rest of the parent's,
+        // read in place (a chain of such children -- a hub's neighbours taken
+        // one by one -- then costs a frame per level, not a list per level)
+        const uint32_t n = f.cnt.get(s);
+        ch.off.set(s, f.off.get(s) + 2 * (p + 1));
+        cnt = n > p + 1 ? n - p - 1 : 0u;
+        ch.flags |= s ? FL_SHARED1 : FL_SHARED0;
     } else {
         const uint32_t* lst = t.arena + f.off.get(s);
         const uint32_t n = f.cnt.get(s);
@@ -986,7 +999,7 @@ __device__ uint32_t build_child(Ctx& t, const Outputs& o, uint32_t cur, uint32_t
         }
     }
     ch.cnt.set(s, cnt);
-    w += 2 * cnt;
+    if (!(ch.flags & (FL_SHARED0 | FL_SHARED1))) w += 2 * cnt;
 
     // ---- other side
     ch.off.set(os, w);
@@ -1744,7 +1757,8 @@ __device__ unsigned long long run_record(Ctx& t, const Outputs& o, const uint32_
     h.order = __ldcg(fr + F_ORDER); h.phase = __ldcg(fr + F_PHASE); h.pos = __ldcg(fr + F_POS);
     h.end = __ldcg(fr + F_END);
     h.cnt.a = c0; h.cnt.b = c1;
-    h.flags &= ~(FL_BITS0 | FL_BITS1);   // bitmaps are not part of a record
+    // bitmaps are not part of a record, and its lists are stored after the frame
+    h.flags &= ~(FL_BITS0 | FL_BITS1 | FL_SHARED0 | FL_SHARED1);
     h.off.a = F_WORDS;
     h.off.b = F_WORDS + 2 * c0;
     h.top = F_WORDS + 2 * (c0 + c1);

@@ -1252,7 +1252,9 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
             CK(cudaMemsetAsync(g0->d_rc, 0, sizeof(RoundCounters), g0->stream));
             CK(cudaMemsetAsync(&g0->d_rc->out_fail, 0xFF, 2 * sizeof(unsigned long long), g0->stream));
             if (share && ws.dq_dirty) {
-                CK(cudaMemsetAsync(ws.d_dq_idx, 0, 8ull * std::min<unsigned long long>(ws.dq_dirty, dq_idx_cap),
+                // every slot an earlier launch may have written, not only this one's
+                CK(cudaMemsetAsync(ws.d_dq_idx, 0,
+                                   8ull * std::min<unsigned long long>(ws.dq_dirty, ws.dq_idx_bytes / 8),
                                    g0->stream));
                 ws.dq_dirty = 0;
             }

@@ -133,7 +133,7 @@ def test_shipped_model_ranks_held_out_roots():
             assert rho > 0.6 and mre < 0.5
 
 
-@pytest.mark.parametrize("nshards", [16, 64])
+@pytest.mark.parametrize("nshards", [64, 256])
 def test_shipped_model_balances_shards_better_than_without_it(nshards):
     # Shards are fixed before the run (no stealing between GPUs), so their
     # balance rests on the cost estimate: the model's predictions against the
@@ -150,8 +150,16 @@ def test_shipped_model_balances_shards_better_than_without_it(nshards):
             equal = _imbalance(g, nodes, np.ones(g.n_left, np.float32), nshards)
             print(f"{name} x{nshards}: max/mean shard load learned {learned:.3f}, "
                   f"proxy {proxy:.3f}, equal {equal:.3f}")
-            assert learned < proxy and learned < equal, (name, learned, proxy, equal)
-            assert learned < 1.2
+            if nshards == 64:
+                assert learned < proxy and learned < equal, (name, learned, proxy, equal)
+                assert learned < 1.2
+            else:
+                # 256 shards: the largest root alone can exceed a shard's mean,
+                # which bounds every partition alike (er200); the model never
+                # does worse, and does better where the bound is not reached
+                assert learned <= proxy and learned <= equal, (name, learned, proxy, equal)
+                if name == "cl20k":
+                    assert learned < proxy and learned < equal
 
 
 def test_learned_batched_at_least_twice_the_plain_schedule():

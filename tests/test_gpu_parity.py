@@ -237,16 +237,26 @@ def test_small_arena_reports_error_not_fault(graphs):
     assert graphs("er60").enumerate(k=1).count == 8041
 
 
-@pytest.mark.parametrize("schedule,arena", [("batched", 160), ("batched", 400), ("plain", 400)])
-def test_paths_that_outgrow_the_arena_move_to_the_next_round(golden, graphs, schedule, arena):
+@pytest.mark.parametrize("schedule", ["batched", "plain"])
+def test_paths_that_outgrow_the_arena_move_to_the_next_round(golden, graphs, schedule):
     # a child (or a node's scratch) that does not fit sends the task's path to
     # the next round, each frame at the bottom of an empty arena: the set is
-    # unchanged and only extra rounds show it
-    for name, k in [("er200", 1), ("southernwomen", 2), ("er60", 2)]:
+    # unchanged and only extra rounds show it.  Arenas from barely two frames
+    # up: every run that succeeds is exact, the rest report GMK_E_ARENA (a
+    # base frame that cannot hold one child), and some succeed after moving
+    # paths (more than one round).
+    moved = 0
+    for name, k in [("er200", 1), ("crime", 1), ("southernwomen", 2), ("er60", 2)]:
         case = next(c for c in golden["cases"] if c["graph"] == name and c["k"] == k)
-        st = graphs(name).enumerate(k=k, arena_words=arena, schedule=schedule)
-        assert st.summary() == _summary(case), (name, k, arena)
-        assert st.rounds > 1
+        for arena in (36, 48, 64, 96, 128, 192):
+            try:
+                st = graphs(name).enumerate(k=k, arena_words=arena, schedule=schedule)
+            except G.GmkError as e:
+                assert e.code == -6, (name, arena, e)
+                continue
+            assert st.summary() == _summary(case), (name, k, arena)
+            moved += st.rounds > 1
+    assert moved > 0
 
 
 def test_watchdog_returns_status():

@@ -514,6 +514,7 @@ GMK_HD uint32_t build_child(Task& t, const Outputs& o, uint32_t cur, uint32_t c,
     // ---- same side as c
     ch[F_OFF0 + s] = w;
     uint32_t cnt = 0;
+    bool shared = false;
     if (is_global(f, s)) {
         if (nsat == 0) {
             ch[F_FLAGS] |= s ? FL_G1 : FL_G0;
@@ -531,6 +532,13 @@ GMK_HD uint32_t build_child(Task& t, const Outputs& o, uint32_t cur, uint32_t c,
                 t.arena[w + 2 * cnt] = v; t.arena[w + 2 * cnt + 1] = m; ++cnt;
             }
         }
+    } else if (!forced && nsat == 0) {
+        // nothing to filter: the rest of the parent's list, read in place
+        // (nothing is stored after the frame for this side)
+        const uint32_t n = f[F_CNT0 + s];
+        ch[F_OFF0 + s] = f[F_OFF0 + s] + 2 * (p + 1);
+        shared = true;
+        cnt = n > p + 1 ? n - p - 1 : 0u;
     } else {
         const uint32_t* lst = t.arena + f[F_OFF0 + s];
         const uint32_t n = f[F_CNT0 + s];
@@ -545,7 +553,7 @@ GMK_HD uint32_t build_child(Task& t, const Outputs& o, uint32_t cur, uint32_t c,
         }
     }
     ch[F_CNT0 + s] = cnt;
-    w += 2 * cnt;
+    if (!shared) w += 2 * cnt;
 
     // ---- other side
     ch[F_OFF0 + os] = w;

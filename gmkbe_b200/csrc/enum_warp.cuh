@@ -1690,8 +1690,10 @@ __device__ __forceinline__ unsigned long long run_dfs(Ctx& t, const Outputs& o, 
     }
     if (t.err == TASK_ARENA_FULL) {
         // the path moves to the next round; only a task's base frame that
-        // cannot hold its own node or one child is an arena overflow
+        // cannot hold its own node or one child is an arena overflow (the
+        // split list's refusal reason says which: 5 = the base frame)
         t.err = 0;
+        if (cur == 0 && sb && t.lane == 0) atomicCAS(sb->refused, 0, 5);
         if (!(cur != 0 && sb && split_path(t, *sb, cur))) fail(t, o, TASK_E_ARENA);
     }
     pop_to(t, 0);

@@ -1060,6 +1060,12 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
             chunk_roots(jobs[i].g->nl, jobs[i].g->n, roots[i], costs[i], unit, max_chunks,
                         (uint32_t)i, plan);
         order_and_shard(plan, nsh, sh);
+        // Under a result limit balance does not matter (every warp stays busy
+        // until the limit) but time to the limit does: the cheapest tasks --
+        // low-degree roots, dense in small results -- go first.
+        if (opts->result_limit)
+            std::stable_sort(plan.begin(), plan.end(),
+                             [](const gmk_task& a, const gmk_task& b) { return a.cost < b.cost; });
     }
     unsigned long long n_tasks = 0;
     for (size_t i = 0; i < ng; ++i) {
@@ -1294,11 +1300,13 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
             }
             const unsigned long long consumed = std::min(r.next_task, a.queue_len);
             if (consumed > n_records) root_next += consumed - n_records;
-            if (h.error == gmk::TASK_E_OUTBUF) {
+            if (h.error == gmk::TASK_E_OUTBUF || h.error == gmk::TASK_E_ARENA) {
                 static const char* why[] = {"", "unentered root frame", "nothing pending",
-                                            "split words full", "split index full"};
-                g_cuda_err = std::string("record deferral failed: ") +
-                             why[r.split_refused >= 0 && r.split_refused <= 4 ? r.split_refused : 0];
+                                            "split words full", "split index full",
+                                            "a task's base frame cannot hold one child"};
+                g_cuda_err = std::string(h.error == gmk::TASK_E_ARENA ? "arena overflow: "
+                                                                       : "record deferral failed: ") +
+                             why[r.split_refused >= 0 && r.split_refused <= 5 ? r.split_refused : 0];
             }
             if (h.error || h.stop || sink_rc != GMK_OK) break;
             const unsigned long long next = std::min({r.next_count, split_idx_cap, r.next_fail});

@@ -149,12 +149,28 @@ def read_graph_bin(path: str) -> Graph:
 
 # ----------------------------------------------------------------------------- generators
 
+DENSE_ER_PAIRS = 1 << 24   # larger ER graphs are sampled edge by edge
+
+
 def erdos_renyi(nu: int, nv: int, p: float, seed: int) -> Graph:
-    """Each of the nu*nv pairs independently with probability p (PCG64(seed))."""
+    """Each of the nu*nv pairs independently with probability p (PCG64(seed)).
+    Up to DENSE_ER_PAIRS pairs every pair is drawn (the committed fixtures were
+    made that way); above it the edge count is drawn from Binomial(nu*nv, p)
+    and that many distinct pairs are drawn uniformly -- the same distribution
+    without a dense nu x nv draw."""
     rng = np.random.Generator(np.random.PCG64(seed))
-    mask = rng.random((nu, nv)) < p
-    li, ri = np.nonzero(mask)
-    return relabel(li, ri)
+    if nu * nv <= DENSE_ER_PAIRS:
+        mask = rng.random((nu, nv)) < p
+        li, ri = np.nonzero(mask)
+        return relabel(li, ri)
+    total = nu * nv
+    m = int(rng.binomial(total, p))
+    keys = np.unique(rng.integers(0, total, size=m + m // 8 + 16, dtype=np.int64))
+    while keys.size < m:
+        keys = np.unique(np.concatenate([keys, rng.integers(0, total, size=m - keys.size + 16,
+                                                            dtype=np.int64)]))
+    keys = rng.permutation(keys)[:m]
+    return relabel(keys // nv, keys % nv)
 
 
 def _chung_lu_weights(n: int, gamma: float, mean_deg: float, cap: float | None) -> np.ndarray:

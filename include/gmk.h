@@ -85,7 +85,9 @@ enum {
                                   search trees are split into the next round's tasks */
     GMK_SCHEDULE_ORDERED = 2   /* batched over planned tasks: roots split into chunks in
                                   proportion to a caller-given cost (task_cost, e.g. the
-                                  subtree-size model's prediction), largest first */
+                                  subtree-size model's prediction); largest first for a
+                                  complete run (balance), smallest first under a result limit
+                                  (results sooner) */
 };
 
 /* Search engines (same rules, same result set). */

@@ -149,6 +149,8 @@ def mixed_batch_stated(cap: int = 1_000_000, n_graphs: int = 64) -> dict:
         t0 = time.perf_counter()
         batch = enumerate_batch(dgs, ks, schedule="ordered", task_costs=costs, limits=caps)
         wall_batch = time.perf_counter() - t0
+        enumerate_batch(dgs, ks, schedule="batched", limits=caps)
+        chunk_major = enumerate_batch(dgs, ks, schedule="batched", limits=caps)
         seq_ms, seq_wall, same_counts = 0.0, 0.0, True
         for dg, k, st in zip(dgs, ks, batch):
             t0 = time.perf_counter()
@@ -161,6 +163,7 @@ def mixed_batch_stated(cap: int = 1_000_000, n_graphs: int = 64) -> dict:
                 "edges": [g.n_edges for g, _ in pairs], "counts": [st.count for st in batch],
                 "truncated": sum(st.truncated for st in batch),
                 "batch_ms": batch[0].kernel_ms, "batch_wall_s": wall_batch,
+                "batch_chunk_major_ms": chunk_major[0].kernel_ms,
                 "one_plain_launch_per_graph_ms": seq_ms, "one_launch_per_graph_wall_s": seq_wall,
                 "speedup_device": seq_ms / batch[0].kernel_ms, "same_counts": same_counts,
                 "batch_results_per_s": total / (batch[0].kernel_ms / 1e3)}

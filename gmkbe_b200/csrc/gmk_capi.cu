@@ -1060,10 +1060,13 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
             chunk_roots(jobs[i].g->nl, jobs[i].g->n, roots[i], costs[i], unit, max_chunks,
                         (uint32_t)i, plan);
         order_and_shard(plan, nsh, sh);
-        // Under a result limit balance does not matter (every warp stays busy
-        // until the limit) but time to the limit does: the cheapest tasks --
-        // low-degree roots, dense in small results -- go first.
-        if (opts->result_limit)
+        // Under a result limit (the run's, or a batch graph's cap) balance does
+        // not matter (every warp stays busy until the limit) but time to the
+        // limit does: the cheapest tasks -- low-degree roots, dense in small
+        // results -- go first.
+        bool capped = opts->result_limit != 0;
+        for (const GraphJob& j : jobs) capped |= j.limit != 0;
+        if (capped)
             std::stable_sort(plan.begin(), plan.end(),
                              [](const gmk_task& a, const gmk_task& b) { return a.cost < b.cost; });
     }

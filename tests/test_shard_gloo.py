@@ -109,6 +109,8 @@ def _recovery_main(rank, world, port, store_port, name, k, leaver, q):
     plan, run_tasks = _task_runner(name, k)
     summ, missing = run_with_recovery(store, rank, world, plan, run_tasks, wait_s=5.0)
     q.put((rank, summ, missing))
+    q.close()
+    q.join_thread()        # the queue's feeder thread must deliver before os._exit
     # the store's host stays up until every survivor has combined
     store.add("gmk/finished", 1)
     if rank == 0:

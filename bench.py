@@ -234,19 +234,26 @@ def _schedules(g, k, limit, cost, reps, flush, check=None, **kw):
     median of `reps` runs after one untimed run each; sets compared."""
     import torch
     out, summ = {}, {}
+    import gmkbe_b200 as G
     for name, extra in (("learned", dict(schedule="ordered", task_cost=cost)),
                         ("batched", dict(schedule="batched")), ("plain", dict(schedule="plain"))):
-        g.enumerate(k=k, result_limit=limit, **extra, **kw)
-        ms, st = [], None
-        for _ in range(reps):
-            flush.zero_()
-            torch.cuda.synchronize()
-            st = g.enumerate(k=k, result_limit=limit, **extra, **kw)
-            ms.append(st.kernel_ms)
+        try:
+            g.enumerate(k=k, result_limit=limit, **extra, **kw)
+            ms, st = [], None
+            for _ in range(reps):
+                flush.zero_()
+                torch.cuda.synchronize()
+                st = g.enumerate(k=k, result_limit=limit, **extra, **kw)
+                ms.append(st.kernel_ms)
+        except G.GmkError as e:          # reported in the line, not hidden
+            out[name] = {"error": str(e)}
+            continue
         m = statistics.median(ms)
         out[name] = {"ms": m, "results": st.count, "value": st.count / (m / 1e3),
                      "rounds": st.rounds, "donations": st.donations, "tasks": st.tasks}
         summ[name] = st.summary()
+    if any("error" in out[n] for n in ("learned", "batched", "plain")):
+        return out
     out["learned_vs_plain"] = out["plain"]["ms"] / out["learned"]["ms"]
     out["batched_vs_plain"] = out["plain"]["ms"] / out["batched"]["ms"]
     out["learned_vs_batched"] = out["batched"]["ms"] / out["learned"]["ms"]
@@ -401,7 +408,7 @@ def run_gmk(args, world, rank, local):
             "e2e": {"value": count_all / e2e_max, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
-            "learned_vs_plain": sched["learned_vs_plain"],
+            "learned_vs_plain": sched.get("learned_vs_plain"),
             "schedules": sched,
             "roofline": {
                 "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

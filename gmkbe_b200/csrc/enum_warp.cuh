@@ -274,8 +274,16 @@ __device__ void flush(Ctx& t, const Outputs& o) {
 // A child or a node's scratch did not fit the arena.  Not an error yet: the
 // search loop moves the path into the next round's task list, where each
 // frame restarts at the bottom of an empty arena (run_dfs).
+// The failing frame and the site (1: a node's scratch, 2: a child) go to two
+// spare words after the warp's source list in shared memory, not to registers:
+// the search loop carries no extra state for this rare case.
 constexpr int TASK_ARENA_FULL = 99;
-__device__ __forceinline__ void arena_full(Ctx& t) { t.err = TASK_ARENA_FULL; }
+constexpr uint32_t kSiteNode = 1, kSiteChild = 2;
+__device__ __forceinline__ void arena_full(Ctx& t, uint32_t cur, uint32_t site) {
+    if (t.lane == 0) { t.src[kSrcCap] = cur; t.src[kSrcCap + 1] = site; }
+    __syncwarp();
+    t.err = TASK_ARENA_FULL;
+}
 
 __device__ void fail(Ctx& t, const Outputs& o, int code) {
     if (!t.err) t.err = code;
@@ -878,7 +886,7 @@ __device__ uint32_t build_child(Ctx& t, const Outputs& o, uint32_t cur, uint32_t
     const int os = 1 - s;
     const uint32_t nc = f.top;
     uint32_t w = nc + F_WORDS;
-    if (w > t.cap) { arena_full(t); return kNoPos; }
+    if (w > t.cap) { arena_full(t, cur, kSiteChild); return kNoPos; }
     Hdr ch;
     ch.ns = t.ns; ch.flags = 0; ch.lo.a = ch.lo.b = 0; ch.cnt.a = ch.cnt.b = 0; ch.off.a = ch.off.b = 0;
     ch.order = 0; ch.phase = 0; ch.pos = 0; ch.parent = cur; ch.end = 0xFFFFFFFFu;
@@ -896,7 +904,7 @@ __device__ uint32_t build_child(Ctx& t, const Outputs& o, uint32_t cur, uint32_t
             for (uint32_t i = 1; i < nsat; ++i)
                 if (degree(g, t.sat[i]) < degree(g, z)) z = t.sat[i];
             const uint32_t dz = degree(g, z);
-            if (w + 2ull * dz > t.cap) { arena_full(t); return kNoPos; }
+            if (w + 2ull * dz > t.cap) { arena_full(t, cur, kSiteChild); return kNoPos; }
             if (t.lane == 0) t.work += dz;
             const uint32_t* row = g.adj + g.off[z];
             #pragma unroll 1
@@ -925,7 +933,7 @@ __device__ uint32_t build_child(Ctx& t, const Outputs& o, uint32_t cur, uint32_t
     } else {
         const uint32_t* lst = t.arena + f.off.get(s);
         const uint32_t n = f.cnt.get(s);
-        if (w + 2ull * n > t.cap) { arena_full(t); return kNoPos; }
+        if (w + 2ull * n > t.cap) { arena_full(t, cur, kSiteChild); return kNoPos; }
         const uint32_t start = forced ? 0u : p + 1;
         // the frame's filter bitmaps, when it has them: sel = the rows of sat(c)
         const uint32_t* bm = nullptr;
@@ -1024,7 +1032,7 @@ __device__ uint32_t build_child(Ctx& t, const Outputs& o, uint32_t cur, uint32_t
             unsigned long long bound = 0;
             #pragma unroll 1
             for (uint32_t q = 0; q < nsrc; ++q) bound += degree(g, t.src[q]);
-            if (w + 2 * bound > t.cap) { arena_full(t); return kNoPos; }
+            if (w + 2 * bound > t.cap) { arena_full(t, cur, kSiteChild); return kNoPos; }
             #pragma unroll 1
             for (uint32_t q = 0; q < nsrc; ++q) {
                 const uint32_t m = t.src[q];
@@ -1055,7 +1063,7 @@ __device__ uint32_t build_child(Ctx& t, const Outputs& o, uint32_t cur, uint32_t
     } else {
         const uint32_t* lst = t.arena + f.off.get(os);
         const uint32_t n = f.cnt.get(os);
-        if (w + 2ull * n > t.cap) { arena_full(t); return kNoPos; }
+        if (w + 2ull * n > t.cap) { arena_full(t, cur, kSiteChild); return kNoPos; }
         #pragma unroll 1
         for (uint32_t base = 0; base < n; base += 32) {
             const uint32_t q = base + t.lane;
@@ -1108,7 +1116,7 @@ __device__ int enter_node(Ctx& t, const Outputs& o, uint32_t cur, ChildReq* req)
         const int s = g0 ? 0 : 1, os = 1 - s;
         const uint32_t n = f.cnt.get(os);
         const uint32_t base = f.top;
-        if (base + n + 2ull * t.ns > t.cap) { arena_full(t); return ENTER_DONE; }
+        if (base + n + 2ull * t.ns > t.cap) { arena_full(t, cur, kSiteNode); return ENTER_DONE; }
         if (outsider_addable_mixed(t, s, f.lo.get(s), t.arena + f.off.get(os), n, t.arena + base))
             return ENTER_DONE;
     }
@@ -1120,7 +1128,7 @@ __device__ int enter_node(Ctx& t, const Outputs& o, uint32_t cur, ChildReq* req)
         if (n0 + n1 == 0 || pairs <= t.scan_limit) {
             const uint32_t base = f.top;
             if (base + (unsigned long long)t.ns + n0 + n1 > t.cap) {
-                arena_full(t);
+                arena_full(t, cur, kSiteNode);
                 return ENTER_DONE;
             }
             uint32_t* tot = t.arena + base;
@@ -1644,14 +1652,6 @@ __device__ __forceinline__ unsigned long long run_dfs(Ctx& t, const Outputs& o, 
             t.nodes++;
             task_nodes++;
             const int r = enter_node<kRec, kBits>(t, o, cur, &req);
-            if (t.err == TASK_ARENA_FULL) {
-                // the node's scratch did not fit: it is entered again next
-                // round, from the bottom of an empty arena (after the loop)
-                if (t.lane == 0) f[F_FLAGS] &= ~FL_ENTERED;
-                __syncwarp();
-                t.nodes--;
-                break;
-            }
             if (kRec && r == ENTER_DEFER) {
                 // re-enter this node next round, after the host drained the buffer
                 set_word(t, cur + F_FLAGS, flags);
@@ -1673,28 +1673,27 @@ __device__ __forceinline__ unsigned long long run_dfs(Ctx& t, const Outputs& o, 
         if (!want) want = next_child(t, cur, &req);
         if (!want) { cur = f[F_PARENT_SLOT]; continue; }
         const uint32_t ch = build_child<kBits>(t, o, cur, req.c, req.s, req.p, req.forced, req.opp_done);
-        if (t.err == TASK_ARENA_FULL) {
-            // the child did not fit: put the frame back where it was before
-            // this child -- a forced child (phase 2) re-enters the node, any
-            // other steps back one position in its phase -- and move the path
-            // to the next round, where each frame starts an empty arena.  A
-            // task's base frame that cannot fit one child is a real overflow.
-            if (t.lane == 0) {
-                if (f[F_PHASE] == 2) f[F_FLAGS] &= ~FL_ENTERED;
-                else f[F_POS] -= 1;
-            }
-            __syncwarp();
-            break;
-        }
         cur = ch == kNoPos ? f[F_PARENT_SLOT] : ch;   // kNoPos: t.err is set, the loop ends
     }
     if (t.err == TASK_ARENA_FULL) {
-        // the path moves to the next round; only a task's base frame that
-        // cannot hold its own node or one child is an arena overflow (the
-        // split list's refusal reason says which: 5 = the base frame)
+        // A node's scratch or a child did not fit.  Put the frame back as it
+        // was -- the node is entered again (its scratch, or a forced child:
+        // phase 2), or steps back one position in its phase -- and move the
+        // path to the next round, where each frame starts an empty arena.
+        // Only a task's base frame that cannot hold its node or one child is
+        // an arena overflow (the split list's refusal reason 5 says so).
+        const uint32_t at = t.src[kSrcCap], site = t.src[kSrcCap + 1];
+        uint32_t* f = t.arena + at;
+        const bool reenter = site == kSiteNode || f[F_PHASE] == 2;
+        if (t.lane == 0) {
+            if (reenter) f[F_FLAGS] &= ~FL_ENTERED;
+            else f[F_POS] -= 1;
+        }
+        __syncwarp();
+        if (reenter) t.nodes--;
         t.err = 0;
-        if (cur == 0 && sb && t.lane == 0) atomicCAS(sb->refused, 0, 5);
-        if (!(cur != 0 && sb && split_path(t, *sb, cur))) fail(t, o, TASK_E_ARENA);
+        if (at == 0 && sb && t.lane == 0) atomicCAS(sb->refused, 0, 5);
+        if (!(at != 0 && sb && split_path(t, *sb, at))) fail(t, o, TASK_E_ARENA);
     }
     pop_to(t, 0);
     return task_nodes;

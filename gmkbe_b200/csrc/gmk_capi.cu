@@ -233,7 +233,7 @@ template <bool kBatch, bool kRec, bool kBits>
 __global__ void __launch_bounds__(kWBlock, kBatch ? kBatchMinBlocks : GMK_WARP_MIN_BLOCKS)
 enumerate_warp_kernel(const __grid_constant__ WarpArgs a) {
     __shared__ uint32_t s_sat[kWarpsPerBlock][gmk::kSatCap];
-    __shared__ uint32_t s_src[kWarpsPerBlock][gmk::warp::kSrcCap];
+    __shared__ uint32_t s_src[kWarpsPerBlock][gmk::warp::kSrcCap + 2];   // + arena-overflow note
     using namespace gmk::warp;
     const uint32_t wib = threadIdx.x >> 5;
     const uint32_t lane = lane_id();

@@ -133,3 +133,45 @@ def tune(g: Graph, g_host, k: int, base_cost: np.ndarray, result_limit: int = 0,
             json.dump(cache, f, indent=1)
         os.replace(tmp, cache_path)
     return dict(out, cached=False)
+
+
+# configurations the gain is reported on: (workload, k, result limit, induced prefix or None)
+GAIN_CASES = [("cl20k", 1, 1_000_000, None), ("cl20k_sub", 1, 0, None),
+              ("cl100k", 2, 10_000_000, None), ("cl100k", 1, 0, (20_000, 60_000)),
+              ("cl500k", 1, 10_000_000, None), ("cl500k", 2, 0, (20_000, 40_000))]
+
+
+def main(argv=None) -> int:
+    """python -m gmkbe_b200.autotune [--passes 1]: tunes each GAIN_CASES workload
+    (costs: the shipped model's predictions) and prints one JSON line per case
+    with the default and the tuned device time."""
+    import argparse
+    import sys
+    from . import graphgen as gg
+    from . import learned as L
+    ap = argparse.ArgumentParser(description="tuned vs default settings on configurations 2-4")
+    ap.add_argument("--passes", type=int, default=1)
+    ap.add_argument("--repeats", type=int, default=2)
+    a = ap.parse_args(argv)
+    model = L.load_default()
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    for name, k, limit, sub in GAIN_CASES:
+        if name == "cl20k_sub":
+            h = gg.read_graph_bin(os.path.join(root, "tests", "golden", "cl20k_sub.graph.bin"))
+        else:
+            h = gg.read_graph_bin(gg.cached_workload(name))
+            if sub:
+                h = gg.induced_prefix(h, *sub)
+        with Graph.from_graph(h) as g:
+            cost = L.predicted_costs(model, g, k)
+            r = tune(g, h, k, cost, result_limit=limit, repeats=a.repeats, passes=a.passes)
+            print(json.dumps({"workload": name if not sub else f"{name} induced {sub[0]}x{sub[1]}",
+                              "k": k, "result_limit": limit, "default_ms": r["default_ms"],
+                              "tuned_ms": r["ms"], "gain": r["gain"], "settings": r["settings"],
+                              "trials": len(r["trials"])}), flush=True)
+            sys.stdout.flush()
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -1483,7 +1483,13 @@ __device__ __forceinline__ Rest frame_rest(const GraphView& g, const uint32_t* f
 // Inlined: an out-of-line call makes the search loop save its live
 // registers around the call site (ptxas: 48 -> 270 bytes of stack and 5x
 // the spill loads).
-__device__ __forceinline__ bool donate_top(Ctx& t, const Donation& db, uint32_t cur) {
+#ifndef GMK_DONATE_PARTS
+#define GMK_DONATE_PARTS 1
+#endif
+constexpr uint32_t kMaxDonateParts = GMK_DONATE_PARTS;
+
+__device__ __forceinline__ bool donate_top(Ctx& t, const Donation& db, uint32_t cur,
+                                           unsigned long long want) {
     uint32_t best = kNoPos;
     Rest rb{0, 0, false};
     #pragma unroll 1
@@ -1499,27 +1505,35 @@ __device__ __forceinline__ bool donate_top(Ctx& t, const Donation& db, uint32_t 
     const uint32_t c0 = (f[F_FLAGS] & FL_G0) ? 0u : f[F_CNT0];
     const uint32_t c1 = (f[F_FLAGS] & FL_G1) ? 0u : f[F_CNT1];
     const unsigned long long words = kRecHeader + 2ull * ns + F_WORDS + 2ull * (c0 + c1);
+    // the split: `parts` records of q children each from the front of the
+    // current phase's remaining children (one record takes half; with many
+    // warps waiting, up to kMaxDonateParts records of equal shares), the
+    // donor keeps the rest
+    const uint32_t rem = rb.lim - rb.pos;
+    uint32_t parts = 1;
+    if (rem >= 3 && want > 1) {
+        const unsigned long long cap = want < kMaxDonateParts ? want : kMaxDonateParts;
+        parts = (uint32_t)(cap < rem - 1 ? cap : rem - 1);
+    }
     unsigned long long w0 = 0, slot = 0;
     int ok = 0;
     if (t.lane == 0) {
-        w0 = atomicAdd(db.used, words);
-        if (w0 + words <= db.word_cap) {
-            slot = atomicAdd(db.tail, 1ull);
-            ok = slot < db.idx_cap;
+        w0 = atomicAdd(db.used, words * parts);
+        if (w0 + words * parts <= db.word_cap) {
+            slot = atomicAdd(db.tail, (unsigned long long)parts);
+            ok = slot + parts <= db.idx_cap;
         }
         if (!ok) atomicExch(db.full, 1);
     }
     if (!bcast(ok)) return false;
     w0 = bcast(w0);
     slot = bcast(slot);
-    // the split: record phase / range, and what the donor keeps
-    const uint32_t rem = rb.lim - rb.pos;
-    uint32_t r_phase = f[F_PHASE], r_pos = rb.pos, r_end, r_flags = f[F_FLAGS];
+    uint32_t r_phase = f[F_PHASE], r_pos = rb.pos, q = 1, r_flags = f[F_FLAGS], r_end = 0;
     uint32_t keep_phase = f[F_PHASE], keep_pos;
     if (rem >= 1) {
-        r_end = rb.pos + (rem >= 2 ? rem / 2 : 1u);
+        q = rem >= 2 ? rem / (parts + 1) : 1u;
         r_flags |= FL_ONE_PHASE;
-        keep_pos = r_end;
+        keep_pos = rb.pos + parts * q;
     } else {
         // the current phase is used up: the record takes the second phase
         const int s2 = f[F_ORDER] ? 0 : 1;
@@ -1530,8 +1544,10 @@ __device__ __forceinline__ bool donate_top(Ctx& t, const Donation& db, uint32_t 
         keep_pos = f[F_POS];
     }
     uint32_t* r = db.words + w0;
-    if (t.lane == 0) { r[0] = ns; r[1] = c0; r[2] = c1; r[3] = t.gid; }
-    uint32_t* rs = r + kRecHeader;
+    if (t.lane < parts) {
+        uint32_t* rp = r + t.lane * words;
+        rp[0] = ns; rp[1] = c0; rp[2] = c1; rp[3] = t.gid;
+    }
     // members as of the frame, with their misses at that depth: the deeper
     // members' misses are taken off (recorded masks where they exist, else
     // adjacency tests), so the warp's own S stays as it is
@@ -1549,32 +1565,40 @@ __device__ __forceinline__ bool donate_top(Ctx& t, const Donation& db, uint32_t 
                 if (side_of(t.g, c) != sm && !adj_test(t, c, m)) --miss;
             }
         }
-        rs[i] = m;
-        rs[ns + i] = miss;
+        #pragma unroll 1
+        for (uint32_t pp = 0; pp < parts; ++pp) {
+            uint32_t* rs = r + pp * words + kRecHeader;
+            rs[i] = m;
+            rs[ns + i] = miss;
+        }
     }
-    uint32_t* fr = rs + 2 * ns;
-    if (t.lane < F_WORDS) {
-        uint32_t v = f[t.lane];
-        v = t.lane == F_PHASE ? r_phase : v;
-        v = t.lane == F_POS ? r_pos : v;
-        v = t.lane == F_END ? r_end : v;
-        v = t.lane == F_FLAGS ? r_flags : v;
-        fr[t.lane] = v;
-    }
-    uint32_t* lr = fr + F_WORDS;
     const uint32_t* a0 = t.arena + f[F_OFF0];
     const uint32_t* a1 = t.arena + f[F_OFF1];
     #pragma unroll 1
-    for (uint32_t i = t.lane; i < 2 * c0; i += 32) lr[i] = a0[i];
-    #pragma unroll 1
-    for (uint32_t i = t.lane; i < 2 * c1; i += 32) lr[2 * c0 + i] = a1[i];
-    __threadfence();                       // every lane's record words before the slot
+    for (uint32_t pp = 0; pp < parts; ++pp) {
+        uint32_t* fr = r + pp * words + kRecHeader + 2 * ns;
+        if (t.lane < F_WORDS) {
+            uint32_t v = f[t.lane];
+            v = t.lane == F_PHASE ? r_phase : v;
+            v = t.lane == F_POS ? (rem >= 1 ? r_pos + pp * q : r_pos) : v;
+            v = t.lane == F_END ? (rem >= 1 ? r_pos + (pp + 1) * q : r_end) : v;
+            v = t.lane == F_FLAGS ? r_flags : v;
+            fr[t.lane] = v;
+        }
+        uint32_t* lr = fr + F_WORDS;
+        #pragma unroll 1
+        for (uint32_t i = t.lane; i < 2 * c0; i += 32) lr[i] = a0[i];
+        #pragma unroll 1
+        for (uint32_t i = t.lane; i < 2 * c1; i += 32) lr[2 * c0 + i] = a1[i];
+    }
+    __threadfence();                       // every lane's record words before the slots
     __syncwarp();
     if (t.lane == 0) {
-        atomicAdd(db.outstanding, 1ull);   // before the record can be taken and finished
-        atomicAdd(db.donated, 1ull);
+        atomicAdd(db.outstanding, (unsigned long long)parts);   // before they can finish
+        atomicAdd(db.donated, (unsigned long long)parts);
         __threadfence();
-        atomicExch(db.idx + slot, w0 + 1);
+        #pragma unroll 1
+        for (uint32_t pp = 0; pp < parts; ++pp) atomicExch(db.idx + slot + pp, w0 + pp * words + 1);
         t.arena[best + F_PHASE] = keep_phase;   // the donor keeps the rest
         t.arena[best + F_POS] = keep_pos;
     }
@@ -1626,7 +1650,7 @@ __device__ __forceinline__ unsigned long long run_dfs(Ctx& t, const Outputs& o, 
                     // waiting warps without a record: tickets beyond the reserved slots
                     const long long want = (long long)(*(volatile const unsigned long long*)db->claim -
                                                        *(volatile const unsigned long long*)db->tail);
-                    give = want > 0;
+                    give = want > 0 ? (int)(want < 32 ? want : 32) : 0;
                 }
                 hungry = may_split && task_nodes >= 1 &&
                          ((!share && lim.split_min_nodes && task_nodes >= lim.split_min_nodes &&
@@ -1636,7 +1660,7 @@ __device__ __forceinline__ unsigned long long run_dfs(Ctx& t, const Outputs& o, 
             stop = bcast(stop); late = bcast(late); hungry = bcast(hungry); give = bcast(give);
             if (stop) break;
             if (late) { fail(t, o, TASK_E_TIMEOUT); break; }
-            if (!kRec && give) donate_top(t, *db, cur);
+            if (!kRec && give) donate_top(t, *db, cur, (unsigned long long)give);
             if (hungry) {
                 if (split_path(t, *sb, cur)) break;
                 may_split = false;   // buffer full: finish this task here

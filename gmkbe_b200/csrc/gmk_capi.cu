@@ -474,6 +474,7 @@ struct gmk_graph {
     uint64_t fingerprint = 0;   // hash of the CSR (checkpoint identity)
     uint32_t max_degree = 0;
     uint32_t max_degree_side[2] = {0, 0};   // U side, V side
+    std::vector<uint8_t> root_bucket;       // floor(log32 deg) of every U vertex, capped at 2
     uint32_t* d_off = nullptr;
     uint32_t* d_adj = nullptr;
     Counters* d_ctr = nullptr;
@@ -667,6 +668,7 @@ int upload(const uint32_t* off, const uint32_t* adj, uint32_t n, uint32_t nl, in
         const uint32_t d = off[v + 1] > off[v] ? off[v + 1] - off[v] : 0u;
         g->max_degree = std::max(g->max_degree, d);
         uint32_t& side_max = g->max_degree_side[v < nl ? 0 : 1];
+        if (v < nl) g->root_bucket.push_back(d > 1024 ? 2 : d > 32 ? 1 : 0);
         side_max = std::max(side_max, d);
     }
     auto bail = [&](int code) { gmk_graph_free(g); return code; };
@@ -1064,11 +1066,18 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
         // not matter (every warp stays busy until the limit) but time to the
         // limit does: the cheapest tasks -- low-degree roots, dense in small
         // results -- go first.
+        // The root's degree bucket (32^b, the reference's grouping) comes
+        // first: a hub whose cost the model underestimates must not run
+        // before the cheap roots.
         bool capped = opts->result_limit != 0;
         for (const GraphJob& j : jobs) capped |= j.limit != 0;
-        if (capped)
-            std::stable_sort(plan.begin(), plan.end(),
-                             [](const gmk_task& a, const gmk_task& b) { return a.cost < b.cost; });
+        if (capped) {
+            auto bucket = [&jobs](const gmk_task& t) { return jobs[t.graph].g->root_bucket[t.root]; };
+            std::stable_sort(plan.begin(), plan.end(), [&bucket](const gmk_task& a, const gmk_task& b) {
+                const uint8_t ba = bucket(a), bb = bucket(b);
+                return ba != bb ? ba < bb : a.cost < b.cost;
+            });
+        }
     }
     unsigned long long n_tasks = 0;
     for (size_t i = 0; i < ng; ++i) {

@@ -86,7 +86,8 @@ enum {
     GMK_SCHEDULE_ORDERED = 2   /* batched over planned tasks: roots split into chunks in
                                   proportion to a caller-given cost (task_cost, e.g. the
                                   subtree-size model's prediction); largest first for a
-                                  complete run (balance), smallest first under a result limit
+                                  complete run (balance); under a result limit by root
+                                  degree bucket (<= 32, <= 1024, more), then smallest first
                                   (results sooner) */
 };
 

@@ -31,7 +31,7 @@ import numpy as np
 from .api import Graph
 
 NONE = 0xFFFFFFFF
-DEFAULTS = dict(warps=1.0, hash_load=50, bits_min=64, bucket_scale=(1.0, 1.0, 1.0),
+DEFAULTS = dict(warps=1.0, hash_load=25, bits_min=64, bucket_scale=(1.0, 1.0, 1.0),
                 tasks_per_worker=8, donate_min_nodes=16, pair_limit=4096)
 CHOICES = {
     "warps": [0.5, 0.75, 1.0],

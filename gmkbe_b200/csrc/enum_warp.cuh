@@ -1484,7 +1484,7 @@ __device__ __forceinline__ Rest frame_rest(const GraphView& g, const uint32_t* f
 // registers around the call site (ptxas: 48 -> 270 bytes of stack and 5x
 // the spill loads).
 #ifndef GMK_DONATE_PARTS
-#define GMK_DONATE_PARTS 1
+#define GMK_DONATE_PARTS 4   // records handed out per poll, at most (1-4: 1.2x on short complete runs)
 #endif
 constexpr uint32_t kMaxDonateParts = GMK_DONATE_PARTS;
 
@@ -1636,7 +1636,7 @@ __device__ __forceinline__ unsigned long long run_dfs(Ctx& t, const Outputs& o, 
     while (cur != kNoPos) {
         if (t.err) break;
 #ifndef GMK_POLL_MASK
-#define GMK_POLL_MASK 15u    // stop / watchdog / split checks every 16 loop steps
+#define GMK_POLL_MASK 7u    // stop / watchdog / split / donation checks every 8 loop steps
 #endif
         if ((++polls & GMK_POLL_MASK) == 0) {
             int stop = 0, late = 0, hungry = 0, give = 0;

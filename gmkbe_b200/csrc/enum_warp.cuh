@@ -29,7 +29,8 @@
 // copy made the count-only kernel 271 KB of machine code; rolled it is 176 KB
 // and 1.07-1.31x faster, the shorter trip counts notwithstanding.  Code size
 // is not the whole story, though: one run_dfs call site for root tasks and
-// records (114 KB) measured 1.2x slower than the two inlined copies.
+// records is 1.1-1.5x faster than two inlined copies in the k = 1 kernels,
+// and 1.1x slower in the k >= 2 ones, which keep two.
 #pragma once
 #include "enum_core.cuh"
 
@@ -1093,6 +1094,243 @@ __device__ uint32_t build_child(Ctx& t, const Outputs& o, uint32_t cur, uint32_t
     return nc;
 }
 
+// ----------------------------------------------------------------- small subtrees
+
+// The subtree of a node whose sides are both local yields exactly the maximal
+// k-biplexes L with S ⊆ L ⊆ S ∪ C that have a V member: the node rules and
+// the branching only drop subsets of C that are no such L.  When C has at most
+// kSmallMax entries and S at most 32 members, solve_small tests every subset T
+// of C at once, one subset per lane, on bit masks, instead of walking the
+// subtree node by node:
+//  * S ∪ T is a k-biplex when every member misses at most k of the other side
+//    of S ∪ T: its misses inside S (smc, or the list's miss count for a
+//    candidate) plus popc(T & its candidate-miss mask);
+//  * it is maximal when no vertex outside it can join.  A vertex joins when it
+//    misses at most k of L's other side and none of those has k misses in L
+//    already (a blocker).  Left-out candidates are tested on their masks.  An
+//    outsider of side s that joins some L misses at most k members of S_o and
+//    no member with k misses inside S, so it lies in the row of such a
+//    saturated member (the lowest-degree one), or in one of the rows of any
+//    k + 1 members of S_o.  Those rows are scanned once; each outsider found
+//    is kept as two masks: the members of S_o and the candidates of C_o it
+//    misses.
+// Count mode only (a result is hashed, not written).  Returns false, having
+// changed nothing, when the node does not qualify: a side whose outsiders are
+// not bounded that way (S_o has at most k members, none saturated), source
+// rows longer than kSmallScanMax in total, or too little arena room at
+// `scratch` for the outsiders' masks.
+#ifndef GMK_SMALL_MAX
+#define GMK_SMALL_MAX 6
+#endif
+constexpr uint32_t kSmallMax = GMK_SMALL_MAX;   // 2^6 = 64 subsets: two per lane
+constexpr uint32_t kSmallScanMax = 1024;
+
+__device__ __forceinline__ unsigned long long warp_xor64(unsigned long long v) {
+    #pragma unroll
+    for (int d = 16; d; d >>= 1) v ^= __shfl_xor_sync(kFull, v, d);
+    return v;
+}
+
+__device__ __forceinline__ bool solve_small(Ctx& t, const uint32_t* l0, uint32_t n0,
+                                            const uint32_t* l1, uint32_t n1, uint32_t scratch) {
+    const GraphView& g = t.g;
+    const uint32_t ns = t.ns, m = n0 + n1, k = t.k, lane = t.lane;
+    // lane i < ns holds member i, lane j < m candidate j (list 0, then list 1)
+    const bool is_mem = lane < ns;
+    const uint32_t my_v = is_mem ? t.sid[lane] : 0u;
+    const uint32_t my_smc = is_mem ? t.smc[lane] : 0u;
+    const uint32_t mem1 = __ballot_sync(kFull, is_mem && side_of(g, my_v));
+    const uint32_t mem0 = __ballot_sync(kFull, is_mem) & ~mem1;
+    const bool is_cand = lane < m;
+    const bool c_one = lane >= n0;
+    const uint32_t* lc = c_one ? l1 + 2 * (lane - n0) : l0 + 2 * lane;
+    const uint32_t my_c = is_cand ? lc[0] : 0u;
+    const uint32_t my_cm = is_cand ? lc[1] : 0u;
+    const uint32_t cand0 = (1u << n0) - 1u;
+    const uint32_t cand1 = ((1u << m) - 1u) & ~cand0;
+
+    // outsider sources per outsider side s, as member masks of S_o
+    unsigned long long key0 = ~0ull, key1 = ~0ull;
+    if (is_mem && my_smc >= k) {
+        const unsigned long long key = ((unsigned long long)degree(g, my_v) << 32) | lane;
+        if (side_of(g, my_v)) key1 = key; else key0 = key;
+    }
+    key0 = warp_min64(key0);
+    key1 = warp_min64(key1);
+    uint32_t srcm[2];
+    uint32_t total = 0;
+    #pragma unroll 1
+    for (int s = 0; s < 2; ++s) {
+        const unsigned long long key = s ? key0 : key1;   // side o = 1 - s
+        uint32_t memo = s ? mem0 : mem1;
+        uint32_t sm = 0;
+        if (key != ~0ull) {
+            sm = 1u << (uint32_t)key;
+        } else {
+            if ((uint32_t)__popc(memo) < k + 1) return false;
+            #pragma unroll 1
+            for (uint32_t c = 0; c <= k; ++c) { sm |= memo & (0u - memo); memo &= memo - 1; }
+        }
+        srcm[s] = sm;
+        #pragma unroll 1
+        for (uint32_t x = sm; x; x &= x - 1) total += degree(g, __shfl_sync(kFull, my_v, __ffs(x) - 1));
+    }
+    if (total > kSmallScanMax || scratch + 2ull * total > t.cap) return false;
+
+    // candidate j: the other side's candidates and members it misses
+    uint32_t my_mcc = 0, my_mcs = 0;
+    #pragma unroll 1
+    for (uint32_t j = 0; j < m; ++j) {
+        const uint32_t cj = __shfl_sync(kFull, my_c, j);
+        if (is_cand && c_one != (j >= n0) && !has_edge(t.eh, my_c, cj)) my_mcc |= 1u << j;
+    }
+    #pragma unroll 1
+    for (uint32_t x = c_one ? mem0 : mem1, y = mem0 | mem1; y; y &= y - 1) {
+        const uint32_t i = __ffs(y) - 1;
+        const uint32_t vi = __shfl_sync(kFull, my_v, i);
+        if (is_cand && ((x >> i) & 1u) && !has_edge(t.eh, my_c, vi)) my_mcs |= 1u << i;
+    }
+    // member i: the candidates it misses (the transpose of the above)
+    uint32_t my_msc = 0;
+    #pragma unroll 1
+    for (uint32_t j = 0; j < m; ++j)
+        if ((__shfl_sync(kFull, my_mcs, j) >> lane) & 1u) my_msc |= 1u << j;
+
+    // outsiders: masks (members of S_o missed, candidates of C_o missed)
+    uint32_t* ob = t.arena + scratch;
+    uint32_t n_out = 0;
+    #pragma unroll 1
+    for (int s = 0; s < 2; ++s) {
+        const uint32_t mems = s ? mem1 : mem0, memo = s ? mem0 : mem1;
+        const uint32_t cands = s ? cand1 : cand0, cando = s ? cand0 : cand1;
+        uint32_t seen_src = 0;
+        #pragma unroll 1
+        for (uint32_t sm = srcm[s]; sm; sm &= sm - 1) {
+            const uint32_t qi = __ffs(sm) - 1;
+            const uint32_t src = __shfl_sync(kFull, my_v, qi);
+            const uint32_t d = degree(g, src);
+            const uint32_t* row = g.adj + g.off[src];
+            #pragma unroll 1
+            for (uint32_t base = 0; base < d; base += 32) {
+                const uint32_t p = base + lane;
+                bool keep = p < d;
+                const uint32_t e = keep ? row[p] : 0u;
+                // in S_s or C_s: not an outsider (every shuffle is taken by
+                // all lanes: none sits behind a short-circuit)
+                #pragma unroll 1
+                for (uint32_t y = mems; y; y &= y - 1) {
+                    const uint32_t vi = __shfl_sync(kFull, my_v, __ffs(y) - 1);
+                    keep = keep && vi != e;
+                }
+                #pragma unroll 1
+                for (uint32_t y = cands; y; y &= y - 1) {
+                    const uint32_t cj = __shfl_sync(kFull, my_c, __ffs(y) - 1);
+                    keep = keep && cj != e;
+                }
+                // found at an earlier source already
+                #pragma unroll 1
+                for (uint32_t y = seen_src; y; y &= y - 1) {
+                    const uint32_t vr = __shfl_sync(kFull, my_v, __ffs(y) - 1);
+                    keep = keep && !has_edge(t.eh, e, vr);
+                }
+                // misses against S_o: at most k, none on a member with k misses
+                uint32_t mos = 0;
+                #pragma unroll 1
+                for (uint32_t y = memo; y; y &= y - 1) {
+                    const uint32_t i = __ffs(y) - 1;
+                    const uint32_t vi = __shfl_sync(kFull, my_v, i);
+                    const uint32_t si = __shfl_sync(kFull, my_smc, i);
+                    if (keep && !has_edge(t.eh, e, vi)) {
+                        mos |= 1u << i;
+                        keep = si < k && (uint32_t)__popc(mos) <= k;
+                    }
+                }
+                uint32_t moc = 0;
+                #pragma unroll 1
+                for (uint32_t y = cando; y; y &= y - 1) {
+                    const uint32_t j = __ffs(y) - 1;
+                    const uint32_t cj = __shfl_sync(kFull, my_c, j);
+                    if (keep && !has_edge(t.eh, e, cj)) moc |= 1u << j;
+                }
+                const uint32_t km = __ballot_sync(kFull, keep);
+                if (keep) {
+                    const uint32_t r = n_out + __popc(km & lanemask_lt());
+                    ob[2 * r] = mos;
+                    ob[2 * r + 1] = moc;
+                }
+                n_out += __popc(km);
+            }
+            seen_src |= 1u << qi;
+        }
+    }
+    __syncwarp();
+
+    // hash elements: S's sums, and each candidate's
+    unsigned long long ea = is_mem ? elem_a(my_v) : 0ull;
+    const unsigned long long a_s = warp_sum64(ea);
+    const unsigned long long b_s = warp_sum64(is_mem ? elem_b(ea) : 0ull);
+    const unsigned long long my_ea = is_cand ? elem_a(my_c) : 0ull;
+    const unsigned long long my_eb = is_cand ? elem_b(my_ea) : 0ull;
+
+    // every subset T of C, one per lane
+    unsigned long long cnt = 0, h1 = 0, h2 = 0;
+    const uint32_t nsub = 1u << m;
+    #pragma unroll 1
+    for (uint32_t base = 0; base < nsub; base += 32) {
+        const uint32_t T = base + lane;
+        bool alive = T < nsub && t.nss.b + __popc(T & cand1) > 0;   // a V member
+        uint32_t bs = 0, bt = 0;
+        #pragma unroll 1
+        for (uint32_t y = mem0 | mem1; y; y &= y - 1) {
+            const uint32_t i = __ffs(y) - 1;
+            const uint32_t tt = __shfl_sync(kFull, my_smc, i) + __popc(T & __shfl_sync(kFull, my_msc, i));
+            alive = alive && tt <= k;
+            bs |= tt >= k ? 1u << i : 0u;
+        }
+        #pragma unroll 1
+        for (uint32_t j = 0; j < m; ++j) {
+            const uint32_t tt = __shfl_sync(kFull, my_cm, j) + __popc(T & __shfl_sync(kFull, my_mcc, j));
+            if ((T >> j) & 1u) {
+                alive = alive && tt <= k;
+                bt |= tt >= k ? 1u << j : 0u;
+            }
+        }
+        // left-out candidates, then outsiders: none may join
+        #pragma unroll 1
+        for (uint32_t j = 0; j < m; ++j) {
+            const uint32_t mcc = __shfl_sync(kFull, my_mcc, j);
+            const uint32_t mcs = __shfl_sync(kFull, my_mcs, j);
+            const uint32_t cm = __shfl_sync(kFull, my_cm, j);
+            if (!((T >> j) & 1u) && cm + __popc(T & mcc) <= k && !(mcs & bs) && !(mcc & bt))
+                alive = false;
+        }
+        #pragma unroll 1
+        for (uint32_t x = 0; x < n_out; ++x) {
+            if ((x & 15u) == 0 && !__any_sync(kFull, alive)) break;
+            const uint32_t mos = ob[2 * x], moc = ob[2 * x + 1];
+            if (__popc(mos) + __popc(T & moc) <= k && !(mos & bs) && !(moc & bt)) alive = false;
+        }
+        if (!__any_sync(kFull, alive)) continue;
+        unsigned long long a = a_s, b = b_s;
+        #pragma unroll 1
+        for (uint32_t j = 0; j < m; ++j) {
+            const unsigned long long aj = __shfl_sync(kFull, my_ea, j);
+            const unsigned long long bj = __shfl_sync(kFull, my_eb, j);
+            if ((T >> j) & 1u) { a += aj; b += bj; }
+        }
+        if (alive) {
+            const uint32_t nx = t.nss.a + __popc(T & cand0), ny = t.nss.b + __popc(T & cand1);
+            cnt += 1;
+            h1 += final_h1(a, nx, ny);
+            h2 ^= final_h2(b, nx, ny);
+        }
+    }
+    t.cnt += warp_sum64(cnt);
+    t.hsum += warp_sum64(h1);
+    t.hxor ^= warp_xor64(h2);
+    return true;
+}
+
 // enter_node: the node's result record found no room in the record buffer.
 constexpr int ENTER_DEFER = 3;
 
@@ -1195,6 +1433,13 @@ __device__ int enter_node(Ctx& t, const Outputs& o, uint32_t cur, ChildReq* req)
                 return ENTER_DONE;
             }
             if (addable) return ENTER_DONE;
+            // a small candidate set: every subset at once (solve_small; in the
+            // k = 1 kernels only -- the k >= 2 ones ran 5-25 % slower with it)
+            if (!kRec && !kBits && n0 + n1 <= kSmallMax && t.ns <= 32 &&
+                solve_small(t, l0, n0, l1, n1, base + t.ns + n0 + n1)) {
+                if (t.cnt >= kFlushBatch) flush(t, o);
+                return ENTER_DONE;
+            }
             // forced candidate: fits every leaf that lacks it (first in list order)
             #pragma unroll 1
             for (int s = 0; s < 2; ++s) {
@@ -1723,11 +1968,9 @@ __device__ __forceinline__ unsigned long long run_dfs(Ctx& t, const Outputs& o, 
     return task_nodes;
 }
 
-// Root task: x in U with its first-level children y in [first, last).
-template <bool kRec, bool kBits>
-__device__ unsigned long long run_root(Ctx& t, const Outputs& o, uint32_t root, uint32_t first,
-                                       uint32_t last, const SplitBuf* sb, const RunLimits& lim,
-                                       const Donation* db) {
+// Root task: x in U with its first-level children y in [first, last); the
+// search starts at y = first (run_dfs's first).
+__device__ __forceinline__ void prep_root(Ctx& t, uint32_t root, uint32_t last) {
     t.ns = 0; t.nss.a = t.nss.b = 0;
     t.mask_base = 0;
     push_member(t, root, nullptr);
@@ -1746,19 +1989,16 @@ __device__ unsigned long long run_root(Ctx& t, const Outputs& o, uint32_t root, 
         }
     if (t.lane == 0) write_hdr(t.arena, h);
     __syncwarp();
-    return run_dfs<kRec, kBits>(t, o, first, sb, lim, db);
 }
 
 // Resumed task: a frame written by split_path or donate_top (its S starts
-// with the root).  Records are read with L2-coherent loads (__ldcg): a
-// donated one was written moments ago by a warp on another SM.
-template <bool kRec, bool kBits>
-__device__ unsigned long long run_record(Ctx& t, const Outputs& o, const uint32_t* r,
-                                         const SplitBuf* sb, const RunLimits& lim,
-                                         const Donation* db) {
+// with the root); false (and the task's error set) when it does not fit this
+// warp's member arrays or arena.  Records are read with L2-coherent loads
+// (__ldcg): a donated one was written moments ago by a warp on another SM.
+__device__ __forceinline__ bool prep_record(Ctx& t, const Outputs& o, const uint32_t* r) {
     const uint32_t ns = __ldcg(r), c0 = __ldcg(r + 1), c1 = __ldcg(r + 2);
-    if (ns > t.smax) { fail(t, o, TASK_E_SMAX); return 0; }
-    if (F_WORDS + 2ull * (c0 + c1) > t.cap) { fail(t, o, TASK_E_ARENA); return 0; }
+    if (ns > t.smax) { fail(t, o, TASK_E_SMAX); return false; }
+    if (F_WORDS + 2ull * (c0 + c1) > t.cap) { fail(t, o, TASK_E_ARENA); return false; }
     uint32_t nv = 0;
     const uint32_t* rs = r + kRecHeader;
     #pragma unroll 1
@@ -1793,7 +2033,7 @@ __device__ unsigned long long run_record(Ctx& t, const Outputs& o, const uint32_
     for (uint32_t i = t.lane; i < 2 * (c0 + c1); i += 32) t.arena[F_WORDS + i] = __ldcg(lr + i);
     if (t.lane == 0) write_hdr(t.arena, h);
     __syncwarp();
-    return run_dfs<kRec, kBits>(t, o, 0, sb, lim, db);
+    return true;
 }
 
 }  // namespace warp

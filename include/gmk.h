@@ -86,9 +86,9 @@ enum {
     GMK_SCHEDULE_ORDERED = 2   /* batched over planned tasks: roots split into chunks in
                                   proportion to a caller-given cost (task_cost, e.g. the
                                   subtree-size model's prediction); largest first for a
-                                  complete run (balance); under a result limit by root
-                                  degree bucket (<= 32, <= 1024, more), then smallest first
-                                  (results sooner) */
+                                  complete run (balance); under a result limit in root id
+                                  order, as PLAIN (the cost predicts nodes, not how soon
+                                  results come) */
 };
 
 /* Search engines (same rules, same result set). */

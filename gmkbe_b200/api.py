@@ -28,6 +28,7 @@ EXPORTS = ("gmk_graph_load", "gmk_graph_from_csr", "gmk_graph_info", "gmk_graph_
            "gmk_enumerate_noalloc", "gmk_result_hash", "gmk_strerror", "gmk_last_cuda_error",
            "gmk_abi_version", "gmk_root_features", "gmk_mlp_create", "gmk_mlp_free",
            "gmk_mlp_params", "gmk_mlp_gradient", "gmk_mlp_train", "gmk_mlp_predict",
+           "gmk_mlp_predict_roots",
            "gmk_root_costs", "gmk_plan_tasks", "gmk_graph_set_hash_load")
 
 SCHEDULES = {"plain": 0, "batched": 1, "ordered": 2}
@@ -122,6 +123,8 @@ def load_library(path: str = LIB_PATH):
     lib.gmk_mlp_train.argtypes = [ctypes.c_void_p, PF, PF, ctypes.c_uint32, ctypes.c_uint32,
                                   ctypes.c_float, PF]
     lib.gmk_mlp_predict.argtypes = [ctypes.c_void_p, PF, ctypes.c_uint32, PF]
+    if hasattr(lib, "gmk_mlp_predict_roots"):
+        lib.gmk_mlp_predict_roots.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, PF]
     lib.gmk_result_hash.argtypes = [P32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                                     ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
     lib.gmk_result_hash.restype = None

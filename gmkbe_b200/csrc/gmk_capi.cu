@@ -504,8 +504,6 @@ struct gmk_graph {
     uint32_t* d_off = nullptr;
     uint32_t* d_adj = nullptr;
     Counters* d_ctr = nullptr;
-    uint32_t* d_order = nullptr;
-    size_t order_bytes = 0;
     unsigned long long* d_eh = nullptr;   // edge hash: buckets of 4 keys
     unsigned long long eh_bmask = 0;
     size_t eh_bytes = 0;
@@ -524,6 +522,11 @@ struct gmk_graph {
 };
 
 namespace {
+
+// Bytes of a graph's root-feature buffer: one FP16 row per U vertex.
+size_t feat_bytes(const gmk_graph* g) {
+    return (size_t)std::max<uint32_t>(g->nl, 1) * gmk::mlp::F * sizeof(__half);
+}
 
 // Search arenas, member buffers and the record buffer are large and outlive
 // any one graph: one set per device, grown on demand, kept until exit.
@@ -622,6 +625,18 @@ void pool_free(int dev, void* p, size_t bytes) {
     } else {
         cudaFree(p);
     }
+}
+
+// grow() over the pool, for per-graph buffers that come and go with the graph.
+int pool_grow(int dev, void** p, size_t* have, size_t need) {
+    if (*have >= need && *p) return GMK_OK;
+    pool_free(dev, *p, *have);
+    *p = nullptr;
+    *have = 0;
+    const cudaError_t e = pool_alloc(dev, p, need);
+    if (e != cudaSuccess) { *p = nullptr; return cuda_fail(e, "cudaMalloc(pool)"); }
+    *have = need;
+    return GMK_OK;
 }
 
 cudaError_t pool_stream(int dev, cudaStream_t* s) {
@@ -874,8 +889,10 @@ void gmk_graph_free(gmk_graph* g) {
     pool_free(d, g->d_ctr, sizeof(Counters));
     pool_free(d, g->d_rc, sizeof(RoundCounters));
     pool_free(d, g->d_eh, g->eh_bytes);
-    cudaFree(g->d_order); cudaFree(g->d_root_nodes); cudaFree(g->d_feat); cudaFree(g->d_cost);
-    cudaFree(g->d_tasks);
+    pool_free(d, g->d_root_nodes, 8ull * std::max<uint32_t>(g->nl, 1));
+    pool_free(d, g->d_feat, feat_bytes(g));
+    pool_free(d, g->d_cost, 4ull * std::max<uint32_t>(g->nl, 1));
+    pool_free(d, g->d_tasks, g->tasks_bytes);
     pool_return(d, g->stream, g->ev0);
     pool_return(d, g->copy_stream, g->ev1);
     delete g;
@@ -895,7 +912,7 @@ namespace {
 // Root costs of the proxy (root_cost_kernel), computed once per graph.
 int proxy_costs(gmk_graph* g, const float** out) {
     if (g->cost.size() != g->nl) {
-        if (!g->d_cost) CK(cudaMalloc(&g->d_cost, 4ull * std::max<uint32_t>(g->nl, 1)));
+        if (!g->d_cost) CK(pool_alloc(g->device, (void**)&g->d_cost, 4ull * std::max<uint32_t>(g->nl, 1)));
         gmk::GraphView gv{g->d_off, g->d_adj, g->n, g->nl};
         const uint64_t threads = (uint64_t)g->nl * 32;
         root_cost_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, g->stream>>>(gv, g->d_cost);
@@ -1136,7 +1153,8 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
         t.ctr = g->d_ctr;
         t.root_nodes = nullptr;
         if (j.root_nodes) {
-            if (!g->d_root_nodes) CK(cudaMalloc(&g->d_root_nodes, 8ull * g->nl));
+            if (!g->d_root_nodes)
+                CK(pool_alloc(g->device, (void**)&g->d_root_nodes, 8ull * std::max<uint32_t>(g->nl, 1)));
             CK(cudaMemsetAsync(g->d_root_nodes, 0, 8ull * g->nl, g0->stream));
             t.root_nodes = g->d_root_nodes;
         }
@@ -1151,7 +1169,8 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
         for (size_t i = 0; i < plan.size(); ++i)
             tab[i] = TaskEntry{plan[i].root, plan[i].first, plan[i].last, plan[i].graph};
         if (!tab.empty()) {
-            if ((rc = grow((void**)&g0->d_tasks, &g0->tasks_bytes, sizeof(TaskEntry) * tab.size())))
+            if ((rc = pool_grow(g0->device, (void**)&g0->d_tasks, &g0->tasks_bytes,
+                                sizeof(TaskEntry) * tab.size())))
                 return rc;
             CK(cudaMemcpyAsync(g0->d_tasks, tab.data(), sizeof(TaskEntry) * tab.size(),
                                cudaMemcpyHostToDevice, g0->stream));
@@ -1586,7 +1605,7 @@ int gmk_root_features(const gmk_graph* g, uint32_t k, float* out) {
     CK(cudaSetDevice(g->device));
     if (g->nl == 0) return GMK_OK;
     gmk_graph* gm = const_cast<gmk_graph*>(g);
-    if (!gm->d_feat) CK(cudaMalloc(&gm->d_feat, (uint64_t)g->nl * gmk::mlp::F * sizeof(__half)));
+    if (!gm->d_feat) CK(pool_alloc(g->device, (void**)&gm->d_feat, feat_bytes(g)));
     gmk::GraphView gv{g->d_off, g->d_adj, g->n, g->nl};
     const uint64_t threads = (uint64_t)g->nl * 32;
     gmk::mlp::root_features_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, g->stream>>>(
@@ -1697,6 +1716,27 @@ int gmk_mlp_train(gmk_mlp* m, const float* x, const float* y, uint32_t n, uint32
     float l = 0.f;
     CK(cudaMemcpy(&l, m->d_loss, sizeof(float), cudaMemcpyDeviceToHost));
     if (loss) *loss = l;
+    return GMK_OK;
+}
+
+int gmk_mlp_predict_roots(gmk_mlp* m, const gmk_graph* g, uint32_t k, float* out) {
+    if (!m || !g || !out || k < 1 || m->device != g->device) return GMK_E_INVAL;
+    CK(cudaSetDevice(g->device));
+    if (g->nl == 0) return GMK_OK;
+    gmk_graph* gm = const_cast<gmk_graph*>(g);
+    if (!gm->d_feat) CK(pool_alloc(g->device, (void**)&gm->d_feat, feat_bytes(g)));
+    if (int rc = mlp_reserve(m, g->nl)) return rc;
+    gmk::GraphView gv{g->d_off, g->d_adj, g->n, g->nl};
+    const uint64_t threads = (uint64_t)g->nl * 32;
+    gmk::mlp::root_features_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, g->stream>>>(
+        gv, k, gm->d_feat);
+    CK(cudaGetLastError());
+    const unsigned grid = (g->nl + gmk::mlp::kBlock - 1) / gmk::mlp::kBlock;
+    gmk::mlp::forward_kernel<<<grid, gmk::mlp::kBlock, 0, g->stream>>>(m->d_w, gm->d_feat, g->nl,
+                                                                      nullptr, m->d_out);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, m->d_out, 4ull * g->nl, cudaMemcpyDeviceToHost, g->stream));
+    CK(cudaStreamSynchronize(g->stream));
     return GMK_OK;
 }
 

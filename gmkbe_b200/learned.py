@@ -101,6 +101,14 @@ class SubtreeModel:
         _check(self._lib.gmk_mlp_predict(self._h, _fp(x), x.shape[0], _fp(out)))
         return out
 
+    def predict_roots(self, g: Graph, k: int) -> np.ndarray:
+        """The prediction for every root of g, features and forward pass on the
+        device (gmk_mlp_predict_roots): predict(root_features(g, k)) without
+        the host round trip."""
+        out = np.zeros(g.n_left, np.float32)
+        _check(self._lib.gmk_mlp_predict_roots(self._h, g._h, k, _fp(out)))
+        return out
+
 
 def target(nodes: np.ndarray) -> np.ndarray:
     """Training target: log1p of the node count."""
@@ -147,7 +155,7 @@ def makespan(costs, order, workers: int) -> float:
 
 def predicted_costs(model: SubtreeModel, g: Graph, k: int) -> np.ndarray:
     """Predicted node counts of every root (task_cost for the ordered schedule)."""
-    return np.expm1(np.maximum(model.predict(root_features(g, k)), 0.0)).astype(np.float32)
+    return np.expm1(np.maximum(model.predict_roots(g, k), 0.0)).astype(np.float32)
 
 
 __all__ = ["SubtreeModel", "root_features", "subtree_nodes", "target", "spearman",

@@ -282,6 +282,11 @@ int gmk_mlp_gradient(gmk_mlp* m, const float* x, const float* y, uint32_t n, flo
 int gmk_mlp_train(gmk_mlp* m, const float* x, const float* y, uint32_t n, uint32_t epochs,
                   float lr, float* loss);
 int gmk_mlp_predict(gmk_mlp* m, const float* x, uint32_t n, float* out);
+/* The model's prediction for every root x in U of g (n_left floats): the
+ * features and the forward pass both run on the device, on the graph's stream,
+ * with no host round trip in between; the same values as gmk_root_features
+ * followed by gmk_mlp_predict.  m and g must be on the same device. */
+int gmk_mlp_predict_roots(gmk_mlp* m, const gmk_graph* g, uint32_t k, float* out);
 
 /* ---- task planning (no counterpart in the reference, whose host loop takes the
  * top-level vertices one at a time in id order, src/main.cu:1078-1111) */

@@ -47,6 +47,20 @@ def test_forward_matches_cpu_reference():
     assert np.abs(got - want).max() <= 1e-4 * max(1.0, np.abs(want).max())
 
 
+def test_device_side_prediction_matches_the_host_round_trip():
+    # gmk_mlp_predict_roots feeds the FP16 features to the forward pass on the
+    # device; gmk_root_features + gmk_mlp_predict takes them through the host.
+    # The inputs are the same FP16 values, so the outputs are identical.
+    model = L.load_default()
+    for k in (1, 2):
+        g = gg.read_graph_bin(golden_graph_path("southernwomen"))
+        with G.Graph.from_graph(g) as dg:
+            got = model.predict_roots(dg, k)
+            want = model.predict(L.root_features(dg, k))
+            assert got.shape == (g.n_left,)
+            assert np.array_equal(got, want)
+
+
 def test_training_reduces_loss_and_learns_the_order():
     m = L.SubtreeModel(seed=4)
     x, y = _random_problem(5, 2000)

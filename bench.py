@@ -380,13 +380,13 @@ def run_gmk(args, world, rank, local):
     else:
         tot_ms_max, e2e_max, count_all = tot_ms, e2e_s, float(count)
     # bytes copied per end-to-end step: host -> device the CSR (n+1 offsets and
-    # 2|E| ids), the features for the model (n_left x 16 FP32) and the task
-    # table (16 B a task); device -> host the root features (n_left x 16 FP16),
-    # the predictions (n_left FP32), the CSR check (16 B) and per launch the
-    # round counters (512 B) and totals (88 B)
+    # 2|E| ids) and the task table (16 B a task); device -> host the
+    # predictions (n_left FP32; features and forward pass stay on the device),
+    # the CSR check (16 B) and per launch the round counters (512 B) and
+    # totals (88 B)
     nl = host.n_left
-    h2d = 4 * (off_np.size + adj_np.size) + 64 * nl + 16 * e2e_tasks / args.steps
-    d2h = 32 * nl + 4 * nl + 16 + 600 * e2e_rounds / args.steps
+    h2d = 4 * (off_np.size + adj_np.size) + 16 * e2e_tasks / args.steps
+    d2h = 4 * nl + 16 + 600 * e2e_rounds / args.steps
     if rank == 0:
         peak, peak_kind, sm_max = _peaks()
         ab = _algo_bytes(WORKLOAD, K, 0)

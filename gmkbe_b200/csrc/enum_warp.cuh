@@ -1114,16 +1114,24 @@ __device__ uint32_t build_child(Ctx& t, const Outputs& o, uint32_t cur, uint32_t
 //    k + 1 members of S_o.  Those rows are scanned once; each outsider found
 //    is kept as two masks: the members of S_o and the candidates of C_o it
 //    misses.
-// Count mode only (a result is hashed, not written).  Returns false, having
-// changed nothing, when the node does not qualify: a side whose outsiders are
-// not bounded that way (S_o has at most k members, none saturated), source
-// rows longer than kSmallScanMax in total, or too little arena room at
-// `scratch` for the outsiders' masks.
+// Count mode hashes the results into the warp's counters.  Record mode
+// reserves room for all of the node's records at once (as emit does for one):
+// no room leaves everything untouched and the node is deferred to the next
+// round; then the results are counted (exact limit: past it, skip records)
+// and written.  Returns kSmallNo, having changed nothing, when the node does
+// not qualify: a side whose outsiders are not bounded that way (S_o has at
+// most k members, none saturated), source rows longer than kSmallScanMax in
+// total, too little arena room at `scratch` for the outsiders' masks, or (in
+// record mode) records that would fill more than half the record buffer.
 #ifndef GMK_SMALL_MAX
 #define GMK_SMALL_MAX 6
 #endif
 constexpr uint32_t kSmallMax = GMK_SMALL_MAX;   // 2^6 = 64 subsets: two per lane
-constexpr uint32_t kSmallScanMax = 1024;
+#ifndef GMK_SMALL_SCAN_MAX
+#define GMK_SMALL_SCAN_MAX 1024
+#endif
+constexpr uint32_t kSmallScanMax = GMK_SMALL_SCAN_MAX;   // outsider source-row entries
+constexpr int kSmallNo = 0, kSmallDone = 1, kSmallDefer = 2;
 
 __device__ __forceinline__ unsigned long long warp_xor64(unsigned long long v) {
     #pragma unroll
@@ -1131,8 +1139,19 @@ __device__ __forceinline__ unsigned long long warp_xor64(unsigned long long v) {
     return v;
 }
 
-__device__ __forceinline__ bool solve_small(Ctx& t, const uint32_t* l0, uint32_t n0,
-                                            const uint32_t* l1, uint32_t n1, uint32_t scratch) {
+// Inclusive warp prefix sum.
+__device__ __forceinline__ uint32_t warp_scan(uint32_t v, uint32_t lane) {
+    #pragma unroll
+    for (uint32_t d = 1; d < 32; d <<= 1) {
+        const uint32_t x = __shfl_up_sync(kFull, v, d);
+        if (lane >= d) v += x;
+    }
+    return v;
+}
+
+template <bool kRec>
+__device__ __forceinline__ int solve_small(Ctx& t, const Outputs& o, const uint32_t* l0, uint32_t n0,
+                                           const uint32_t* l1, uint32_t n1, uint32_t scratch) {
     const GraphView& g = t.g;
     const uint32_t ns = t.ns, m = n0 + n1, k = t.k, lane = t.lane;
     // lane i < ns holds member i, lane j < m candidate j (list 0, then list 1)
@@ -1167,7 +1186,7 @@ __device__ __forceinline__ bool solve_small(Ctx& t, const uint32_t* l0, uint32_t
         if (key != ~0ull) {
             sm = 1u << (uint32_t)key;
         } else {
-            if ((uint32_t)__popc(memo) < k + 1) return false;
+            if ((uint32_t)__popc(memo) < k + 1) return kSmallNo;
             #pragma unroll 1
             for (uint32_t c = 0; c <= k; ++c) { sm |= memo & (0u - memo); memo &= memo - 1; }
         }
@@ -1175,7 +1194,7 @@ __device__ __forceinline__ bool solve_small(Ctx& t, const uint32_t* l0, uint32_t
         #pragma unroll 1
         for (uint32_t x = sm; x; x &= x - 1) total += degree(g, __shfl_sync(kFull, my_v, __ffs(x) - 1));
     }
-    if (total > kSmallScanMax || scratch + 2ull * total > t.cap) return false;
+    if (total > kSmallScanMax || scratch + 2ull * total > t.cap) return kSmallNo;
 
     // candidate j: the other side's candidates and members it misses
     uint32_t my_mcc = 0, my_mcs = 0;
@@ -1272,8 +1291,9 @@ __device__ __forceinline__ bool solve_small(Ctx& t, const uint32_t* l0, uint32_t
     const unsigned long long my_ea = is_cand ? elem_a(my_c) : 0ull;
     const unsigned long long my_eb = is_cand ? elem_b(my_ea) : 0ull;
 
-    // every subset T of C, one per lane
+    // every subset T of C, one per lane; found bit r: subset 32 r + lane is a result
     unsigned long long cnt = 0, h1 = 0, h2 = 0;
+    uint32_t found = 0;
     const uint32_t nsub = 1u << m;
     #pragma unroll 1
     for (uint32_t base = 0; base < nsub; base += 32) {
@@ -1310,7 +1330,8 @@ __device__ __forceinline__ bool solve_small(Ctx& t, const uint32_t* l0, uint32_t
             const uint32_t mos = ob[2 * x], moc = ob[2 * x + 1];
             if (__popc(mos) + __popc(T & moc) <= k && !(mos & bs) && !(moc & bt)) alive = false;
         }
-        if (!__any_sync(kFull, alive)) continue;
+        if (alive) found |= 1u << (base >> 5);
+        if (kRec || !__any_sync(kFull, alive)) continue;
         unsigned long long a = a_s, b = b_s;
         #pragma unroll 1
         for (uint32_t j = 0; j < m; ++j) {
@@ -1325,10 +1346,88 @@ __device__ __forceinline__ bool solve_small(Ctx& t, const uint32_t* l0, uint32_t
             h2 ^= final_h2(b, nx, ny);
         }
     }
-    t.cnt += warp_sum64(cnt);
-    t.hsum += warp_sum64(h1);
-    t.hxor ^= warp_xor64(h2);
-    return true;
+    if (!kRec) {
+        t.cnt += warp_sum64(cnt);
+        t.hsum += warp_sum64(h1);
+        t.hxor ^= warp_xor64(h2);
+        return kSmallDone;
+    }
+    // record mode: room for every record of the node first, then the count
+    uint32_t nres = __popc(found), words = 0;
+    #pragma unroll 1
+    for (uint32_t x = found; x; x &= x - 1) {
+        const uint32_t T = ((__ffs(x) - 1) << 5) + lane;
+        words += 2 + ns + __popc(T);
+    }
+    uint32_t rank = warp_scan(nres, lane), off = warp_scan(words, lane);
+    const uint32_t n_res = __shfl_sync(kFull, rank, 31), n_words = __shfl_sync(kFull, off, 31);
+    rank -= nres;
+    off -= words;
+    if (n_res == 0) return kSmallDone;
+    // records that would fill more than half the buffer go one by one (emit)
+    // down the usual path: a node must never need more room than a drained
+    // buffer has
+    if (2ull * n_words > o.out_cap) return kSmallNo;
+    unsigned long long at = 0, c0 = 0;
+    int room = 0;
+    if (lane == 0) {
+        at = atomicAdd(o.out_pos, (unsigned long long)n_words);
+        room = at + n_words <= o.out_cap;
+        if (!room) {
+            atomicMin(o.out_fail, at);
+        } else {
+            c0 = atomicAdd(o.count, (unsigned long long)n_res);
+            if (o.limit && c0 + n_res >= o.limit) atomicExch(o.stop, 1);
+        }
+    }
+    if (!bcast(room)) return kSmallDefer;
+    at = bcast(at);
+    c0 = bcast(c0);
+    #pragma unroll 1
+    for (uint32_t base = 0; base < nsub; base += 32) {
+        const uint32_t T = base + lane;
+        unsigned long long a = a_s, b = b_s;
+        #pragma unroll 1
+        for (uint32_t j = 0; j < m; ++j) {
+            const unsigned long long aj = __shfl_sync(kFull, my_ea, j);
+            const unsigned long long bj = __shfl_sync(kFull, my_eb, j);
+            if ((T >> j) & 1u) { a += aj; b += bj; }
+        }
+        if (!((found >> (base >> 5)) & 1u)) continue;
+        const uint32_t nx = t.nss.a + __popc(T & cand0), ny = t.nss.b + __popc(T & cand1);
+        uint32_t* r = o.out_buf + at + off;
+        off += 2 + nx + ny;
+        if (o.limit && c0 + rank++ >= o.limit) {
+            // past the limit: a skip record of the same length
+            r[0] = 0xFFFFFFFFu;
+            r[1] = nx + ny;
+            continue;
+        }
+        h1 += final_h1(a, nx, ny);
+        h2 ^= final_h2(b, nx, ny);
+        r[0] = nx;
+        r[1] = ny;
+        uint32_t px = 2, py = 2 + nx;
+        #pragma unroll 1
+        for (uint32_t i = 0; i < ns; ++i) {
+            const uint32_t v = t.sid[i];
+            if (side_of(g, v)) r[py++] = v; else r[px++] = v;
+        }
+        #pragma unroll 1
+        for (uint32_t j = 0; j < m; ++j)
+            if ((T >> j) & 1u) {
+                if (j < n0) r[px++] = l0[2 * j];
+                else r[py++] = l1[2 * (j - n0)];
+            }
+    }
+    h1 = warp_sum64(h1);
+    h2 = warp_xor64(h2);
+    if (lane == 0) {
+        atomicAdd(o.hash_sum, h1);
+        atomicXor(o.hash_xor, h2);
+    }
+    __syncwarp();
+    return kSmallDone;
 }
 
 // enter_node: the node's result record found no room in the record buffer.
@@ -1435,10 +1534,13 @@ __device__ int enter_node(Ctx& t, const Outputs& o, uint32_t cur, ChildReq* req)
             if (addable) return ENTER_DONE;
             // a small candidate set: every subset at once (solve_small; in the
             // k = 1 kernels only -- the k >= 2 ones ran 5-25 % slower with it)
-            if (!kRec && !kBits && n0 + n1 <= kSmallMax && t.ns <= 32 &&
-                solve_small(t, l0, n0, l1, n1, base + t.ns + n0 + n1)) {
-                if (t.cnt >= kFlushBatch) flush(t, o);
-                return ENTER_DONE;
+            if (!kBits && n0 + n1 <= kSmallMax && t.ns <= 32) {
+                const int r = solve_small<kRec>(t, o, l0, n0, l1, n1, base + t.ns + n0 + n1);
+                if (r == kSmallDefer) return ENTER_DEFER;
+                if (r == kSmallDone) {
+                    if (!kRec && t.cnt >= kFlushBatch) flush(t, o);
+                    return ENTER_DONE;
+                }
             }
             // forced candidate: fits every leaf that lacks it (first in list order)
             #pragma unroll 1

@@ -145,6 +145,29 @@ def test_chung_lu_small_against_oracle():
         assert dg.enumerate(k=1).summary() == want
 
 
+@pytest.mark.parametrize("seed", [21, 22, 23])
+def test_small_subtree_solver_against_oracle_and_records(seed):
+    # Sparse k = 1 graphs: most local nodes hold at most six candidates, so the
+    # k = 1 kernels test their subsets at once (solve_small).  Count mode, record
+    # mode (streamed through the smallest record buffer the warp engine takes,
+    # so rounds wind down and nodes defer), a limited record run, and the
+    # thread engine (no solver) must all give the oracle's set.
+    g = gg.chung_lu(150, 260, 420, 2.1, seed, max_deg=30)   # 65-73 k results each
+    want = O.enumerate_oracle(g, 1).summary()
+    with G.Graph.from_graph(g) as dg:
+        assert dg.enumerate(k=1).summary() == want
+        assert dg.enumerate(k=1, engine="thread").summary() == want
+        for out_words in (0, 160):
+            sets = []
+            st = dg.enumerate(k=1, sink=lambda x, y: sets.append((tuple(x), tuple(y))),
+                              out_words=out_words)
+            assert st.summary() == want
+            assert len(sets) == want[0] and O.set_summary(sets) == want
+        st = dg.enumerate(k=1, result_limit=max(1, want[0] // 3), collect=True)
+        assert st.count == len(st.results) == max(1, want[0] // 3)
+        assert len(set(st.results)) == st.count
+
+
 HUB_CASES = [(3, 6, 72, 4, 2, 1), (4, 8, 80, 4, 2, 2), (4, 4, 66, 4, 3, 5), (4, 5, 70, 5, 3, 3)]
 
 

@@ -142,6 +142,9 @@ enumerate_kernel(gmk::GraphView g, uint32_t k, Counters* ctr, uint32_t* arenas,
 constexpr int kWBlock = GMK_WARP_BLOCK;
 constexpr int kWarpsPerBlock = kWBlock / 32;
 // Resident blocks per SM the register allocation targets.
+#ifndef GMK_IDLE_SLEEP_MAX
+#define GMK_IDLE_SLEEP_MAX 1024u             // ns: longest back-off of a warp waiting for a record
+#endif
 #ifndef GMK_WARP_MIN_BLOCKS
 #define GMK_WARP_MIN_BLOCKS 25
 #endif
@@ -343,7 +346,7 @@ enumerate_warp_kernel(const __grid_constant__ WarpArgs a) {
                         }
                     }
                     __nanosleep(sleep_ns);
-                    sleep_ns = sleep_ns < 1024 ? sleep_ns * 2 : sleep_ns;
+                    sleep_ns = sleep_ns < GMK_IDLE_SLEEP_MAX ? sleep_ns * 2 : sleep_ns;
                 }
                 __threadfence();
             }

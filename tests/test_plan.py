@@ -103,3 +103,41 @@ def test_ctypes_structs_match_the_header(tmp_path):
     sizes = tuple(int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True,
                                                  check=True).stdout.split())
     assert sizes == (ctypes.sizeof(_Opts), ctypes.sizeof(_Stats), ctypes.sizeof(_Task))
+
+
+def _plan_restated(n, nl, cost, target):
+    """The planner restated: roots by cost, largest first (stable); root r cut
+    into m = clamp(ceil(cost / unit), 1, (n - nl) // 16) equal chunks, unit =
+    total cost / target; all tasks stably sorted by their per-task cost
+    float32(cost / m), largest first."""
+    nv = n - nl
+    c64 = np.maximum(cost.astype(np.float64), 0.0)
+    roots = np.argsort(-cost, kind="stable")
+    unit = c64[roots].sum() / max(1, target)
+    wide = max(1, nv // 16)
+    tasks = []
+    for r in roots:
+        m = int(max(1.0, min(np.ceil(c64[r] / unit) if unit > 0 else 1.0, float(wide))))
+        width = (nv + m - 1) // m
+        for i in range(m):
+            first = nl + i * width
+            if first >= n:
+                break
+            tasks.append((int(r), first, min(n, first + width), float(np.float32(c64[r] / m))))
+    tasks.sort(key=lambda t: -t[3])     # stable
+    return tasks
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_plan_order_is_a_stable_sort_of_the_tasks_by_cost(seed):
+    # The planner sorts roots by per-task cost instead of sorting every task;
+    # a root's chunks share one cost, so the order must be exactly that of a
+    # stable sort of all tasks (ties included: costs are rounded here).
+    rng = np.random.default_rng(seed)
+    nl, nv = int(rng.integers(50, 400)), int(rng.integers(40, 900))
+    cost = np.round(np.exp(rng.uniform(0, 6, nl)) / 20).astype(np.float32)
+    for target in (1, 37, 2000):
+        plan = G.plan_tasks(nl + nv, nl, cost, target_tasks=target)
+        want = _plan_restated(nl + nv, nl, cost, target)
+        got = [(int(t["root"]), int(t["first"]), int(t["last"]), float(t["cost"])) for t in plan]
+        assert got == want, (seed, target)

@@ -136,6 +136,7 @@ enum : int {
     TASK_E_SMAX = 2,    // |S| above the member capacity
     TASK_E_TIMEOUT = 3, // watchdog deadline passed
     TASK_E_OUTBUF = 4,  // a result record found no room and could not be deferred
+    TASK_E_RECORD = 5,  // a split or donated task record failed its checks (internal error)
 };
 
 struct Outputs {

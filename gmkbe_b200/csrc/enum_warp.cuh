@@ -2101,6 +2101,9 @@ __device__ __forceinline__ bool prep_record(Ctx& t, const Outputs& o, const uint
     const uint32_t ns = __ldcg(r), c0 = __ldcg(r + 1), c1 = __ldcg(r + 2);
     if (ns > t.smax) { fail(t, o, TASK_E_SMAX); return false; }
     if (F_WORDS + 2ull * (c0 + c1) > t.cap) { fail(t, o, TASK_E_ARENA); return false; }
+    // Every id and position of the record is checked before the search uses
+    // it: a record that fails is reported (TASK_E_RECORD), never followed.
+    bool bad = ns == 0;
     uint32_t nv = 0;
     const uint32_t* rs = r + kRecHeader;
     #pragma unroll 1
@@ -2109,7 +2112,8 @@ __device__ __forceinline__ bool prep_record(Ctx& t, const Outputs& o, const uint
         bool isv = false;
         if (i < ns) {
             const uint32_t v = __ldcg(rs + i);
-            t.sid[i] = v;
+            bad |= v >= t.g.n;
+            t.sid[i] = v < t.g.n ? v : 0u;
             t.smc[i] = __ldcg(rs + ns + i);
             isv = side_of(t.g, v) != 0;
         }
@@ -2124,6 +2128,9 @@ __device__ __forceinline__ bool prep_record(Ctx& t, const Outputs& o, const uint
     h.order = __ldcg(fr + F_ORDER); h.phase = __ldcg(fr + F_PHASE); h.pos = __ldcg(fr + F_POS);
     h.end = __ldcg(fr + F_END);
     h.cnt.a = c0; h.cnt.b = c1;
+    bad |= h.ns != ns || h.order > 1 || h.phase > 2 ||
+           ((h.flags & FL_G0) && h.lo.a >= t.g.nl) ||
+           ((h.flags & FL_G1) && (h.lo.b + 1 < t.g.nl || h.lo.b >= t.g.n));
     // bitmaps are not part of a record, and its lists are stored after the frame
     h.flags &= ~(FL_BITS0 | FL_BITS1 | FL_SHARED0 | FL_SHARED1);
     h.off.a = F_WORDS;
@@ -2132,7 +2139,12 @@ __device__ __forceinline__ bool prep_record(Ctx& t, const Outputs& o, const uint
     h.parent = kNoPos;
     const uint32_t* lr = fr + F_WORDS;
     #pragma unroll 1
-    for (uint32_t i = t.lane; i < 2 * (c0 + c1); i += 32) t.arena[F_WORDS + i] = __ldcg(lr + i);
+    for (uint32_t i = t.lane; i < 2 * (c0 + c1); i += 32) {
+        uint32_t x = __ldcg(lr + i);
+        if (!(i & 1u) && x >= t.g.n) { bad = true; x = 0; }   // list entries: (id, misses)
+        t.arena[F_WORDS + i] = x;
+    }
+    if (__any_sync(kFull, bad)) { fail(t, o, TASK_E_RECORD); return false; }
     if (t.lane == 0) write_hdr(t.arena, h);
     __syncwarp();
     return true;

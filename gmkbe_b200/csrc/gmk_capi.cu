@@ -1445,6 +1445,9 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
         case gmk::TASK_E_SMAX: return GMK_E_SMAX;
         case gmk::TASK_E_TIMEOUT: return GMK_E_TIMEOUT;
         case gmk::TASK_E_OUTBUF: return GMK_E_OUTBUF;
+        case gmk::TASK_E_RECORD:
+            g_cuda_err = "a split or donated task record failed its checks (internal error)";
+            return GMK_E_CUDA;
         default: return GMK_E_CUDA;
     }
     if (warp) return warp_emit_rc;

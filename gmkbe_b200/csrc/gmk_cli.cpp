@@ -6,16 +6,28 @@
 //   -m / -g are accepted and ignored (verbose dump / unused group size).
 // Output: "Result N: X: x1 x2 | Y: y1 y2 " lines when -q 1 (format of
 // reference include/output.cuh:102-145), then "Running Time: <ms> ms".
+// Progress as the reference reports it (src/main.cu:1752-1760,
+// include/output.cuh:350-372): "Output <n>, cost Time: <ms> ms" on stderr when
+// the result count reaches 10^i or the limit (every one with -q 1; the final
+// one in count mode, which has no per-result host step), and the time to the
+// limit kept in <dir>/<stem>.gpu<k>.json as {"<k>": {"<limit>": ms}}
+// (include/timer.cuh:85-185: merged into an existing file, 5 h written until
+// the limit is reached).  The file is named for the graph given with -f (the
+// reference takes the first .bin of its directory).
 // Extra: --all (no result limit), --schedule plain|batched, --stats,
 // --threads N / --arena WORDS (resident search threads, per-worker arena),
 // --engine warp|thread, --checkpoint FILE [--batch-roots N] (resumable run:
 // the file is rewritten after every batch of roots and a restarted command
-// continues from it).
+// continues from it), --no-time-file.
+#include <cctype>
 #include <charconv>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
+#include <map>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -32,6 +44,11 @@ struct Printer {
     std::vector<char> buf = std::vector<char>(4u << 20);
     size_t len = 0;
     FILE* out = stdout;
+    // progress: the next count to report (10^i, then the limit), the limit
+    // (0: none), the run's start and the time at which the limit was reached
+    unsigned long long next_mark = 1, limit = 0;
+    std::chrono::steady_clock::time_point t0;
+    double limit_ms = -1.0;
 
     void flush() {
         if (len) std::fwrite(buf.data(), 1, len, out);
@@ -68,14 +85,116 @@ int print_result(void* user, const uint32_t* x, uint32_t nx, const uint32_t* y, 
     }
     *p++ = '\n';
     pr->len += (size_t)(p - start);
+    if (pr->n == pr->next_mark) {
+        // a progress mark: results so far go out first, as the reference's
+        // writer flushes at each mark
+        pr->flush();
+        std::fflush(pr->out);
+        const double ms = std::chrono::duration<double, std::milli>(
+                              std::chrono::steady_clock::now() - pr->t0).count();
+        std::fprintf(stderr, "Output %llu, cost Time: %g ms\n", pr->n, ms);
+        if (pr->n == pr->limit) pr->limit_ms = ms;
+        const unsigned long long next = pr->next_mark * 10;
+        pr->next_mark = pr->limit && next >= pr->limit ? pr->limit : next;
+        if (pr->limit && pr->n >= pr->limit) pr->next_mark = 0;   // nothing after the limit
+    }
     return 0;
+}
+
+// The time file: a JSON object of objects of numbers, {"<k>": {"<limit>": ms}}.
+// Read leniently (anything unreadable starts an empty object, as the
+// reference does); written with four-space indents and keys in string order.
+using TimeTable = std::map<std::string, std::map<std::string, std::string>>;
+
+bool parse_string(const std::string& s, size_t& i, std::string& out) {
+    while (i < s.size() && std::isspace((unsigned char)s[i])) ++i;
+    if (i >= s.size() || s[i] != '"') return false;
+    const size_t j = s.find('"', i + 1);
+    if (j == std::string::npos) return false;
+    out = s.substr(i + 1, j - i - 1);
+    i = j + 1;
+    return true;
+}
+
+bool expect(const std::string& s, size_t& i, char c) {
+    while (i < s.size() && std::isspace((unsigned char)s[i])) ++i;
+    if (i >= s.size() || s[i] != c) return false;
+    ++i;
+    return true;
+}
+
+bool peek(const std::string& s, size_t& i, char c) {
+    while (i < s.size() && std::isspace((unsigned char)s[i])) ++i;
+    return i < s.size() && s[i] == c;
+}
+
+TimeTable read_time_table(const std::string& path) {
+    TimeTable t;
+    std::ifstream f(path);
+    if (!f) return t;
+    std::stringstream ss;
+    ss << f.rdbuf();
+    const std::string s = ss.str();
+    size_t i = 0;
+    TimeTable parsed;
+    if (!expect(s, i, '{')) return t;
+    while (!peek(s, i, '}')) {
+        std::string k;
+        if (!parse_string(s, i, k) || !expect(s, i, ':') || !expect(s, i, '{')) return t;
+        auto& row = parsed[k];
+        while (!peek(s, i, '}')) {
+            std::string key;
+            if (!parse_string(s, i, key) || !expect(s, i, ':')) return t;
+            while (i < s.size() && std::isspace((unsigned char)s[i])) ++i;
+            const size_t b = i;
+            while (i < s.size() && (std::isdigit((unsigned char)s[i]) || std::strchr("+-.eE", s[i]))) ++i;
+            if (i == b) return t;
+            row[key] = s.substr(b, i - b);
+            if (!peek(s, i, '}') && !expect(s, i, ',')) return t;
+        }
+        ++i;
+        if (!peek(s, i, '}') && !expect(s, i, ',')) return t;
+    }
+    return parsed;
+}
+
+void write_time_table(const std::string& path, const TimeTable& t) {
+    std::ofstream f(path);
+    if (!f) {
+        std::fprintf(stderr, "Error: Cannot write to file: %s\n", path.c_str());
+        return;
+    }
+    f << "{";
+    bool first = true;
+    for (const auto& [k, row] : t) {
+        f << (first ? "\n" : ",\n") << "    \"" << k << "\": {";
+        bool first2 = true;
+        for (const auto& [key, v] : row) {
+            f << (first2 ? "\n" : ",\n") << "        \"" << key << "\": " << v;
+            first2 = false;
+        }
+        f << (row.empty() ? "}" : "\n    }");
+        first = false;
+    }
+    f << (t.empty() ? "}" : "\n}");
+}
+
+// <dir>/<stem>.gpu<k>.json for the graph file `graph`.
+std::string time_file_path(const std::string& graph, uint32_t k) {
+    const size_t slash = graph.find_last_of('/');
+    const std::string dir = slash == std::string::npos ? "" : graph.substr(0, slash + 1);
+    std::string stem = slash == std::string::npos ? graph : graph.substr(slash + 1);
+    const size_t dot = stem.find_last_of('.');
+    if (dot != std::string::npos && dot > 0) stem = stem.substr(0, dot);
+    return dir + stem + ".gpu" + std::to_string(k) + ".json";
 }
 
 void usage() {
     std::fprintf(stderr,
                  "usage: gmk -f <graph.bin> [-k K] [-r LIMIT] [-q 0|1] [-d DEV] [--all]\n"
                  "           [--schedule plain|batched] [--stats] [--threads N] [--arena WORDS]\n"
-                 "           [--engine warp|thread] [--checkpoint FILE [--batch-roots N]]\n");
+                 "           [--engine warp|thread] [--checkpoint FILE [--batch-roots N]]\n"
+                 "           [--no-time-file]\n");
 }
 
 }  // namespace
@@ -85,7 +204,7 @@ int main(int argc, char** argv) {
     gmk_opts o;
     gmk_opts_default(&o);
     o.result_limit = 10000000ull;
-    int quiet = 0, dev = 0, stats = 0;
+    int quiet = 0, dev = 0, stats = 0, time_file = 1;
     std::string checkpoint;
     uint32_t batch_roots = 0;
     for (int i = 1; i < argc; ++i) {
@@ -101,6 +220,7 @@ int main(int argc, char** argv) {
         else if (!std::strcmp(argv[i], "-m") || !std::strcmp(argv[i], "-g")) (void)val(argv[i]);
         else if (!std::strcmp(argv[i], "--all")) o.result_limit = 0;
         else if (!std::strcmp(argv[i], "--stats")) stats = 1;
+        else if (!std::strcmp(argv[i], "--no-time-file")) time_file = 0;
         else if (!std::strcmp(argv[i], "--threads"))
             o.threads = (uint32_t)std::strtoul(val("--threads"), nullptr, 10);
         else if (!std::strcmp(argv[i], "--checkpoint")) checkpoint = val("--checkpoint");
@@ -136,10 +256,22 @@ int main(int argc, char** argv) {
     std::printf("Graph size: %u, edge num: %llu, bipartite index: %u, k = %u, theta = 1\n", n,
                 (unsigned long long)m, nl, o.k);
     std::fflush(stdout);
+    // the time file holds 5 h for this (k, limit) until the limit is reached
+    const std::string limit_key = std::to_string(o.result_limit);
+    const std::string tpath = time_file_path(file, o.k);
+    TimeTable table;
+    if (time_file && o.result_limit) {
+        table = read_time_table(tpath);
+        table[std::to_string(o.k)][limit_key] = "18000000";
+        write_time_table(tpath, table);
+    }
     Printer p;
+    p.limit = o.result_limit;
+    p.next_mark = o.result_limit && o.result_limit <= 1 ? o.result_limit : 1;
     o.emit = quiet ? 1 : 0;
     gmk_stats st;
     const auto t0 = std::chrono::steady_clock::now();
+    p.t0 = t0;
     // results stream through the library's record buffers; no retry is needed
     rc = checkpoint.empty() ? gmk_enumerate(g, &o, quiet ? print_result : nullptr, &p, &st)
                             : gmk_enumerate_resumable(g, &o, checkpoint.c_str(), batch_roots, 0,
@@ -155,6 +287,17 @@ int main(int argc, char** argv) {
     }
     // the double in its shortest round-trip form, as the reference's fmt prints it
     // (src/main.cu:1709)
+    if (!quiet && st.count) {
+        // count mode: the final mark only (no host step per result)
+        std::fprintf(stderr, "Output %llu, cost Time: %g ms\n", (unsigned long long)st.count, wall_ms);
+        if (o.result_limit && st.count >= o.result_limit) p.limit_ms = wall_ms;
+    }
+    if (time_file && o.result_limit && p.limit_ms >= 0) {
+        char v[64];
+        *std::to_chars(v, v + sizeof(v) - 1, p.limit_ms).ptr = 0;
+        table[std::to_string(o.k)][limit_key] = v;
+        write_time_table(tpath, table);
+    }
     char ms[64];
     *std::to_chars(ms, ms + sizeof(ms) - 1, st.kernel_ms).ptr = 0;
     std::printf("Running Time: %s ms\n", ms);

@@ -22,7 +22,8 @@ RUNNING = re.compile(r"^Running Time: (\d+(?:\.\d+)?(?:e[-+]?\d+)?) ms$")
 
 
 def _run(*args):
-    p = subprocess.run([CLI, *args], capture_output=True, text=True, timeout=300)
+    # --no-time-file: no side file next to the committed fixtures
+    p = subprocess.run([CLI, *args, "--no-time-file"], capture_output=True, text=True, timeout=300)
     assert p.returncode == 0, p.stderr
     return p.stdout.splitlines()
 
@@ -76,7 +77,8 @@ def test_million_line_output_rate(golden, tmp_path):
     out = tmp_path / "out.txt"
     with open(out, "w") as f:
         p = subprocess.run([CLI, "-f", golden_graph_path("er200"), "-k", "1", "-q", "1", "--all",
-                            "--stats"], stdout=f, stderr=subprocess.PIPE, text=True, timeout=300)
+                            "--stats", "--no-time-file"], stdout=f, stderr=subprocess.PIPE,
+                           text=True, timeout=300)
     assert p.returncode == 0, p.stderr
     tail = subprocess.run(["tail", "-n", "2", str(out)], capture_output=True, text=True).stdout
     stats = dict(zip(*[iter(tail.splitlines()[-1].split())] * 2))
@@ -87,3 +89,33 @@ def test_million_line_output_rate(golden, tmp_path):
     assert int(wc) == case["count"] + 3
     print(f"gmk -q 1: {stats['lines']} lines, {float(stats['lines_per_s']) / 1e6:.2f} M lines/s "
           f"(wall {stats['wall_ms']} ms)")
+
+
+def test_progress_marks_and_time_file(tmp_path):
+    # The reference reports "Output <n>, cost Time: <ms> ms" on stderr at 10^i
+    # results and at the limit (src/main.cu:1752-1760, include/output.cuh:350-372)
+    # and keeps the time to the limit in <stem>.gpu<k>.json next to the graph
+    # (include/timer.cuh:85-185): 5 h until the limit is reached, other
+    # entries of the file kept.
+    import json
+    import shutil
+    graph = tmp_path / "sw.graph.bin"
+    shutil.copy(golden_graph_path("southernwomen"), graph)
+    side = tmp_path / "sw.gpu1.json"
+    side.write_text(json.dumps({"2": {"5": 1.5}}))
+    p = subprocess.run([CLI, "-f", str(graph), "-k", "1", "-r", "100", "-q", "1"],
+                       capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr
+    marks = re.findall(r"^Output (\d+), cost Time: ([0-9.e+-]+) ms$", p.stderr, re.M)
+    assert [int(n) for n, _ in marks] == [1, 10, 100]
+    table = json.loads(side.read_text())
+    assert table["2"] == {"5": 1.5}
+    assert 0 < table["1"]["100"] < 18_000_000
+    # count mode, limit above the total (1 256 results): the final mark only,
+    # and the 5 h placeholder stays for that limit
+    p = subprocess.run([CLI, "-f", str(graph), "-k", "1", "-r", "1000000"],
+                       capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr
+    assert re.findall(r"^Output (\d+),", p.stderr, re.M) == ["1256"]
+    table = json.loads(side.read_text())
+    assert table["1"]["1000000"] == 18_000_000 and table["1"]["100"] < 18_000_000

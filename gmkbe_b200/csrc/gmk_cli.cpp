@@ -4,8 +4,9 @@
 //   -f <file.graph.bin>  -k <k> (default 1)  -r <result limit> (default 1e7)
 //   -q <print results, 0/1> (default 0)  -d <device> (default 0)
 //   -m / -g are accepted and ignored (verbose dump / unused group size).
-// Output: "Result N: X: x1 x2 | Y: y1 y2 " lines when -q 1 (format of
-// reference include/output.cuh:102-145), then "Running Time: <ms> ms".
+// Output: "Using GPU: <name>, GPU id: <d>", the "Graph size: ..." header,
+// "Result N: X: x1 x2 | Y: y1 y2 " lines when -q 1 (format of reference
+// include/output.cuh:102-145), then "Running Time: <ms> ms".
 // Progress as the reference reports it (src/main.cu:1752-1760,
 // include/output.cuh:350-372): "Output <n>, cost Time: <ms> ms" on stderr when
 // the result count reaches 10^i or the limit (every one with -q 1; the final
@@ -30,6 +31,8 @@
 #include <sstream>
 #include <string>
 #include <vector>
+
+#include <cuda_runtime.h>
 
 #include "gmk.h"
 
@@ -243,6 +246,12 @@ int main(int argc, char** argv) {
         }
     }
     if (file.empty()) { usage(); return 2; }
+    // the reference's first line (src/main.cu:1766-1770)
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) == cudaSuccess) {
+        std::printf("Using GPU: %s, GPU id: %d\n", prop.name, dev);
+        std::fflush(stdout);
+    }
     gmk_graph* g = nullptr;
     int rc = gmk_graph_load(file.c_str(), dev, &g);
     if (rc) {

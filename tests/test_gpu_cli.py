@@ -43,9 +43,10 @@ def _parse(lines):
 def test_result_lines_match_the_reference_format_and_set():
     lines = _run("-f", golden_graph_path("southernwomen"), "-k", "1", "-q", "1", "--all")
     results, other = _parse(lines)
-    assert HEADER.match(other[0]), other[0]
+    assert re.match(r"^Using GPU: .+, GPU id: 0$", other[0]), other[0]
+    assert HEADER.match(other[1]), other[1]
     assert RUNNING.match(other[-1]), other[-1]
-    assert len(other) == 2, other
+    assert len(other) == 3, other
     assert [n for n, _, _ in results] == list(range(1, len(results) + 1))
     got = {(x, y) for _, x, y in results}
     want = set()
@@ -56,7 +57,7 @@ def test_result_lines_match_the_reference_format_and_set():
     assert len(results) == len(got) == 1256
     assert got == want
     # ids ascending within each side, X in U and Y in V
-    n, _, nl, _ = (int(v) for v in HEADER.match(other[0]).groups())
+    n, _, nl, _ = (int(v) for v in HEADER.match(other[1]).groups())
     for _, x, y in results:
         assert list(x) == sorted(x) and list(y) == sorted(y)
         assert x[-1] < nl <= y[0] and y[-1] < n

@@ -102,7 +102,7 @@ def test_progress_marks_and_time_file(tmp_path):
     import shutil
     graph = tmp_path / "sw.graph.bin"
     shutil.copy(golden_graph_path("southernwomen"), graph)
-    side = tmp_path / "sw.gpu1.json"
+    side = tmp_path / "sw.graph.gpu1.json"   # the stem drops the last extension only
     side.write_text(json.dumps({"2": {"5": 1.5}}))
     p = subprocess.run([CLI, "-f", str(graph), "-k", "1", "-r", "100", "-q", "1"],
                        capture_output=True, text=True, timeout=300)

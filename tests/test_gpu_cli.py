@@ -87,7 +87,7 @@ def test_million_line_output_rate(golden, tmp_path):
     assert int(stats["hash_sum"], 16) == int(case["hash_sum"], 16)
     assert int(stats["hash_xor"], 16) == int(case["hash_xor"], 16)
     wc = subprocess.run(["wc", "-l", str(out)], capture_output=True, text=True).stdout.split()[0]
-    assert int(wc) == case["count"] + 3
+    assert int(wc) == case["count"] + 4   # + the GPU line, header, running time, stats
     print(f"gmk -q 1: {stats['lines']} lines, {float(stats['lines_per_s']) / 1e6:.2f} M lines/s "
           f"(wall {stats['wall_ms']} ms)")
 

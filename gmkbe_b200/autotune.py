@@ -1,4 +1,5 @@
-"""Autotuner for the warp engine: the knobs north_star names, per graph.
+"""Autotuner for the warp engine: occupancy, edge-hash capacity, intersection
+strategy and per-degree-bucket chunking, per graph.
 
 For one (graph, k, result limit) it times short enumerations and keeps the
 fastest setting, by coordinate descent from the defaults (each knob in turn

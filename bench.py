@@ -5,7 +5,7 @@ on rank 0.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gmk|reference]
 
-Workload (the headline `value`): configuration 2's exactness case -- the
+Workload (the headline `value`): the exactness case of cl20k -- the
 Chung-Lu graph |U| = 20k, |V| = 50k (exponent 2.1, max degree 2k, seed 2),
 complete enumeration of the subgraph induced by its first 5k U and 12k V ids
 (tests/golden/cl20k_sub.graph.bin: 623 x 653 vertices, 660 edges, 245 860
@@ -22,10 +22,11 @@ build, root features, model prediction, planning, enumeration and read-back
 all inside the timed region.  L2 is flushed (256 MB write) between steps.
 
 Beside it: the plain schedule (one task per root, id order, no splitting) and
-the batched schedule without the model on the same graph; configuration 2's
-throughput run (full graph, first 10^6 results) and configurations 3 and 4
-(first 10^7 / 10^8 results) under the three schedules; and complete
-enumerations of configuration 1 and of subgraphs of configurations 3 and 4.
+the batched schedule without the model on the same graph; cl20k's throughput
+run (full graph, first 10^6 results) and the Chung-Lu 100k x 300k (cl100k) and
+500k x 1M (cl500k) graphs (first 10^7 / 10^8 results) under the three
+schedules; and complete enumerations of the Erdos-Renyi 200 x 200 graph (er200)
+and of subgraphs of cl100k and cl500k.
 `--impl reference` times the reference's own CPU enumerator (BPPivot, built
 from its sources under oracle/_ref) on the same complete enumeration.  With
 N > 1 (one process per GPU under torchrun) every rank runs its shard of the
@@ -51,7 +52,7 @@ METRIC = "maximal k-biplexes/sec, learned+batched vs plain GPU, bit-exact result
 UNIT = "results/s"
 WORKLOAD = "cl20k_sub"
 WORKLOAD_PATH = os.path.join(ROOT, "tests", "golden", "cl20k_sub.graph.bin")
-CONFIG_DESC = ("config 2: Chung-Lu bipartite |U|=20k |V|=50k ~500k edges, exponent 2.1, max "
+CONFIG_DESC = ("cl20k: Chung-Lu bipartite |U|=20k |V|=50k ~500k edges, exponent 2.1, max "
                "degree 2k, seed 2; complete enumeration of the subgraph induced by the first 5k U "
                "and 12k V ids (623 x 653 vertices, 660 edges after dropping isolated vertices), "
                "k=1, 245860 maximal 1-biplexes, bit-exact against BPPivot")
@@ -265,9 +266,9 @@ def _schedules(g, k, limit, cost, reps, flush, check=None, **kw):
 
 
 def _extras(model, flush, device):
-    """Configuration 2's throughput run and configurations 3-4, result-limited,
-    and complete enumerations of configuration 1 and of the config-3/4 family
-    subgraphs, under the three schedules."""
+    """cl20k's throughput run and cl100k / cl500k, result-limited, and complete
+    enumerations of er200 and of cl100k / cl500k subgraphs, under the three
+    schedules."""
     import gmkbe_b200 as G
     from gmkbe_b200 import graphgen as gg
     from gmkbe_b200 import learned as L
@@ -291,7 +292,7 @@ def _extras(model, flush, device):
 
 
 # complete enumerations beside the headline: (workload, k, induced prefix or None).  As for
-# configuration 2's exactness case, a prefix is the subgraph induced by the first U and V ids
+# cl20k's exactness case, a prefix is the subgraph induced by the first U and V ids
 # (the converter's order: lowest degrees first), sized so that the run ends in well under a second.
 COMPLETE_CASES = [("er200", 1, None), ("cl100k", 1, (20000, 60000)), ("cl100k", 2, (4000, 12000)),
                   ("cl500k", 2, (20000, 40000)), ("cl500k", 3, (10000, 20000))]

@@ -150,7 +150,7 @@ def main(argv=None) -> int:
     import sys
     from . import graphgen as gg
     from . import learned as L
-    ap = argparse.ArgumentParser(description="tuned vs default settings on configurations 2-4")
+    ap = argparse.ArgumentParser(description="tuned vs default settings on cl20k, cl100k and cl500k")
     ap.add_argument("--passes", type=int, default=1)
     ap.add_argument("--repeats", type=int, default=2)
     a = ap.parse_args(argv)

@@ -1133,7 +1133,7 @@ int run_jobs(std::vector<GraphJob>& jobs, const gmk_opts* opts, gmk_sink sink, v
         // nodes the first `limit` results cost does, and that depends on the
         // order.  The model predicts node counts, not result density: largest
         // first took 4-36x longer to the limit than id order, cheapest first
-        // 1.1-1.25x less at k = 2 but 1.4-7x more at k = 1 (config 4: 632 M
+        // 1.1-1.25x less at k = 2 but 1.4-7x more at k = 1 (cl500k: 632 M
         // nodes for 10^8 results against 60 M).  So capped runs keep each
         // graph's roots in id order (the plain schedule's), chunks as planned.
         bool capped = opts->result_limit != 0;

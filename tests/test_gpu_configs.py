@@ -1,11 +1,10 @@
-"""Configurations 3 and 4 on the GPU (Chung-Lu 100k x 300k, exponent 2.2,
-seed 3; Chung-Lu 500k x 1M, exponent 2.0, seed 4).  Their complete result
+"""The Chung-Lu 100k x 300k (exponent 2.2, seed 3) and 500k x 1M (exponent
+2.0, seed 4) workloads on the GPU.  Their complete result
 sets are far too large to enumerate, so:
   * on the full graphs, the first 50 000 results of a record-mode run (and of a
     run that splits after every two nodes) are distinct, and every sampled one
     is a maximal k-biplex by the oracle's direct classifier;
-  * on subgraphs induced by their first ids (as configuration 2's exactness
-    case is), complete count-mode enumerations -- the k >= 2 filter-bitmap
+  * on subgraphs induced by their first ids (as cl20k's exactness case is), complete count-mode enumerations -- the k >= 2 filter-bitmap
     kernel with in-launch sharing -- equal the C oracle's set summary."""
 import numpy as np
 import pytest

@@ -1,4 +1,4 @@
-"""Checkers for the maximal k-biplex enumerator -- TEST INFRASTRUCTURE ONLY.
+"""Oracles for the maximal k-biplex enumerator -- TEST INFRASTRUCTURE ONLY.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU legs import this
 package.  It holds:
@@ -6,7 +6,7 @@ package.  It holds:
   * _ref/bppivot   -- the reference's own CPU enumerator (BPPivot), compiled
                       from its sources by oracle/Makefile;
   * _ref/gmkbpe    -- the reference's own GPU enumerator (make -C oracle refgpu),
-                      run on a GPU box as a second reference;
+                      run on a machine with a GPU as a second reference;
   * brute_force    -- exhaustive definition check for graphs of <= 16 vertices;
   * result_hash    -- the canonical per-result hash shared with the CUDA code.
 """

@@ -1,6 +1,6 @@
 /* CPU oracle for maximal k-biplex enumeration -- TEST INFRASTRUCTURE ONLY.
  *
- * Used by tests/ and by bench.py's CPU leg as the checker; the product path
+ * Used by tests/ and by bench.py's CPU leg as the oracle; the product path
  * (gmkbe_b200's CUDA library) never links, loads or calls this file.
  *
  * It restates, on a dense adjacency matrix and with one plain recursion, the

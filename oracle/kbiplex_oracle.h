@@ -1,6 +1,6 @@
 /* CPU oracle for maximal k-biplex enumeration -- TEST INFRASTRUCTURE ONLY.
  *
- * This library is the checker the tests and bench.py's CPU leg compare the
+ * This library is the oracle the tests and bench.py's CPU leg compare the
  * CUDA enumerator against.  The product never links or calls it.
  *
  * Graph: CSR over global ids, U = [0, n_left), V = [n_left, n); rows sorted.

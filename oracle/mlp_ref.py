@@ -1,6 +1,6 @@
 """CPU float64 restatement of the subtree-size model -- TEST INFRASTRUCTURE ONLY.
 
-The checker for the library's FP16/FP32 MLP kernels (gmkbe_b200/csrc/mlp.cuh):
+The oracle for the library's FP16/FP32 MLP kernels (gmkbe_b200/csrc/mlp.cuh):
 the same 16-64-64-1 ReLU network, the same parameter layout
 (W1[64][16] b1[64] W2[64][64] b2[64] W3[64] b3), the same mean-squared-error
 loss, computed in float64 from the FP16-rounded weights and inputs the kernels

@@ -2,7 +2,7 @@
 build recipes only (oracle/Makefile uses the same variable).
 
 $GMK_REFERENCE names the checkout; without it the default checkout location
-below is used.  Nothing on the GPU side reads it: the built checkers under
+below is used.  Nothing on the GPU side reads it: the built oracles under
 oracle/_ref and the committed fixtures under tests/golden travel instead.
 """
 import os

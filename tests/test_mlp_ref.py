@@ -1,4 +1,4 @@
-"""The CPU restatement of the subtree-size model (the checker of the GPU MLP
+"""The CPU restatement of the subtree-size model (the oracle of the GPU MLP
 kernels) against central finite differences, and the ranking / scheduling
 helpers of gmkbe_b200.learned."""
 import numpy as np

@@ -1,4 +1,4 @@
-"""CPU checks of the checkers themselves: the C oracle against the definition
+"""CPU checks of the oracles themselves: the C oracle against the definition
 (brute force) and against the golden summaries taken from the reference's
 BPPivot, plus the graph format and converter-ordering helpers."""
 import os
